@@ -1,0 +1,302 @@
+"""Benchmark: wall-clock / biological-time ratio of a 1e9-synapse Brunel network on one B200
+(the reference's headline, README.md:39 / samples/main.cpp:1337-1369: 100,000 steps of
+0.1 ms = 10 s of biological time, setup excluded).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One bench "step" = 1,050 simulation steps (0.105 s biological, 70 windows of delay 15),
+run through the public API (spk_net_run); the default K = 96 covers 10.08 s biological.
+The 4.15 GB synapse table is far larger than L2, so no flush is needed between steps.
+With N > 1 (torchrun), every rank simulates its own independent replica (the path does
+not shard across GPUs on the single-GPU scope); value = max wall over ranks / total
+biological time simulated by all ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+POPS = [70710, 70710]                 # N = sqrt(1e9 / 0.05) = 141,420 (samples/main.cpp:1283,1395)
+CONNS = [(0, 1, 0.1), (1, 1, 0.1)]
+DT, DELAY = 1e-4, 15
+SIM_STEPS = 1050                      # per bench step
+METRIC = "wall/bio time ratio at 1e9-syn Brunel"
+CPU_SAMPLE_STEPS = 120                # reference CPU sample (about 10-30 s on one core)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=96)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return rank, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples (SM clock, max clock, throttle reasons) during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 9 for i in range(4) if s[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the window kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "window_counts_brunel_1e9.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_launch_full_size"])
+    except Exception:
+        return None
+
+
+def cpu_baseline():
+    """The reference's cpu::snn (oracle/_ref, built with the reference's own -O2 -ffast-math)
+    on the same Brunel 1e9 net, one core, a bounded sample of steps after the first `delay`
+    steps (when the spike queue is full). Falls back to the CPU restatement (kind "port")
+    where the reference build is absent. Returns (wall/bio, kind, cores, sample text)."""
+    t0 = time.perf_counter()
+    net, kind = make_cpu_net()
+    setup = time.perf_counter() - t0
+    for _ in range(DELAY):
+        net.step()
+    t0 = time.perf_counter()
+    spikes = 0
+    for _ in range(CPU_SAMPLE_STEPS):
+        spikes += len(net.step())
+    wall = time.perf_counter() - t0
+    del net
+    ratio = wall / (CPU_SAMPLE_STEPS * DT)
+    sample = (f"Brunel 1e9 (N=141,420, width 7,328), {CPU_SAMPLE_STEPS} steps after the first {DELAY} "
+              f"({CPU_SAMPLE_STEPS * DT * 1e3:.0f} ms biological, {spikes} spikes), single thread, setup {setup:.1f} s excluded")
+    return ratio, kind, 1, sample
+
+
+REF_SIM_STEPS = 20  # simulation steps timed per reference-arm bench step
+
+
+def make_cpu_net():
+    import oracle
+
+    if oracle.have_reference(fast=True):
+        return oracle.ReferenceNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, fast=True), "reference"
+    return oracle.OracleNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, graph="reference", graph_seed=1337), "port"
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU simulator on the same workload, rank 0 only: each bench step
+    times REF_SIM_STEPS steps of one constructed net (setup excluded, like the reference)."""
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    net, kind = make_cpu_net()
+    setup = time.perf_counter() - t0
+    for _ in range(DELAY):
+        net.step()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        for _ in range(REF_SIM_STEPS):
+            net.step()
+        if i >= args.warmup:
+            vals.append((time.perf_counter() - t) / (REF_SIM_STEPS * DT))
+    value = statistics.median(vals) if vals else None
+    sample = (f"Brunel 1e9 (N=141,420), {REF_SIM_STEPS} steps per bench step x {args.steps}, single thread "
+              f"(cpu::snn has no threading), setup {setup:.1f} s excluded")
+    line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * REF_SIM_STEPS * DT * 1e3 if value else None,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "brunel_1e9", "neurons": sum(POPS), "synapses": 1e9, "dt": DT, "delay": DELAY,
+                       "model": "brunel"},
+            "cpu_baseline": {"value": value, "unit": "wall_s/bio_s", "cores": 1, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    from spice_b200 import Layout, Snn
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    net = Snn("brunel", Layout(POPS, CONNS), dt=DT, delay=DELAY, seed=1 + rank, graph_seed=1337 + rank, device=dev)
+    net.sync()
+    setup_s = time.perf_counter() - t0
+    info = net.info()
+    stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+    S = args.sim_steps
+    windows_per_step = -(-S // DELAY)
+
+    for _ in range(args.warmup):
+        net.run(S)
+    net.sync()
+    # spike rate from a recorded (untimed) sample, for the algorithmic byte count
+    counts, _ = net.run_record(S)
+    spikes_per_step = float(np.mean(counts))
+    net.sync()
+
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        net.run(S)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+
+    # end to end through the C ABI: spike raster of every bench step to host memory
+    e2e_vals, d2h = [], []
+    for _ in range(max(1, min(args.steps, 10))):
+        t = time.perf_counter()
+        c, ids = net.run_record(S)
+        e2e_vals.append(time.perf_counter() - t)
+        d2h.append(c.nbytes + ids.nbytes)
+    e2e_wall = max_over_ranks(statistics.median(e2e_vals), world)
+    net.close()
+
+    bio = args.steps * S * DT
+    value = (ms_max / 1e3) / (bio * world)
+    # roofline of the window kernel (the only kernel of the timed region)
+    mean_degree = sum(p * (d1 - d0) for (s, d, p), (d0, d1) in zip(CONNS, [(POPS[0], POPS[0] + POPS[1])] * 2))
+    n = sum(POPS)
+    state_bytes = 8  # V, Twait
+    bytes_per_step = spikes_per_step * mean_degree * 4 + spikes_per_step * info.num_tiles * 8
+    bytes_per_window = DELAY * bytes_per_step + 2 * n * state_bytes
+    launches = args.steps * windows_per_step
+    t_launch = (ms / 1e3) / launches
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_window / t_launch / 1e9
+    traffic = profile_traffic()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "brunel_1e9", "neurons": n, "synapses": 1e9, "ell_width": info.width,
+                           "dt": DT, "delay": DELAY, "model": "brunel", "sim_steps_per_bench_step": S,
+                           "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (4.15 GB synapse table)",
+                           "tiles": info.num_tiles, "tile_size": info.tile_size, "setup_s": setup_s,
+                           "spikes_per_step": spikes_per_step},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "traffic": traffic, "peak_kind": peak_kind, "kernel": "window_counts<brunel>",
+                             "bytes_per_launch": bytes_per_window, "launch_us": t_launch * 1e6},
+                "e2e": {"value": e2e_wall / (S * DT * world), "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": int(statistics.median(d2h))},
+                "gpu_launches": launches, "clocks": clk}
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                v, kind, cores, sample = cpu_baseline()
+                line["cpu_baseline"] = {"value": v, "unit": "wall_s/bio_s", "cores": cores, "kind": kind, "sample": sample}
+            except Exception as e:  # report, never fail the GPU line
+                line["cpu_baseline"] = {"value": None, "unit": "wall_s/bio_s", "cores": 1, "kind": "reference",
+                                        "sample": f"unavailable: {e}"}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world = dist_init(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/* spice_b200 -- C ABI of the B200 simulation path.
+ *
+ * A C-ABI shared library (libspice_b200.so) over hand-written sm_100a kernels. The C++17
+ * class template spice::cuda::snn<Model> (include/spice/cuda/snn.h) is a thin wrapper over
+ * these calls, and the Python package spice_b200 binds them with ctypes. Every function
+ * returns an spk_status; on failure spk_last_error() holds a message (per host thread).
+ * Nothing here takes or returns torch types, C++ objects or CUDA handles other than a
+ * cudaStream_t passed as void*.
+ */
+#ifndef SPICE_B200_H
+#define SPICE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum spk_status
+{
+	SPK_OK = 0,
+	SPK_ERR_INVALID = 1,  /* bad argument (the reference throws std::invalid_argument)      */
+	SPK_ERR_CUDA = 2,     /* CUDA runtime error (the reference throws std::runtime_error)    */
+	SPK_ERR_NOMEM = 3,    /* device allocation failed (the reference throws std::bad_alloc)  */
+	SPK_ERR_DEVICE = 4,   /* a kernel reported an error through the net's device error word */
+	SPK_ERR_CAPACITY = 5  /* an output buffer is too small; *count tells the size needed    */
+} spk_status;
+
+typedef enum spk_model
+{
+	SPK_VOGELS_ABBOTT = 0, /* spice/models/vogels_abbott.h          */
+	SPK_BRUNEL = 1,        /* spice/models/brunel.h                 */
+	SPK_BRUNEL_PLUS = 2,   /* spice/models/brunel_with_plasticity.h */
+	SPK_SYNTH = 3          /* spice/models/synth.h                  */
+} spk_model;
+
+/* Population sizes and (src_pop, dst_pop, p) connection list: the arguments of
+ * spice::util::layout(pops, connections) (spice/util/layout.h:30-33). */
+typedef struct spk_layout_desc
+{
+	int npops;
+	uint64_t const * pops;
+	int nconn;
+	int const * conn_src;
+	int const * conn_dst;
+	float const * conn_p;
+} spk_layout_desc;
+
+typedef struct spk_net spk_net;
+
+typedef struct spk_net_info
+{
+	int model;
+	int device;
+	uint64_t num_neurons;  /* snn::num_neurons()  (spice/snn.h:24)                       */
+	uint64_t num_synapses; /* snn::num_synapses() = num_neurons * width (spice/snn.h:25) */
+	uint64_t width;        /* ELL row width = layout::max_degree()                      */
+	int delay;             /* snn::delay()  (spice/snn.h:27)                             */
+	float dt;              /* snn::dt()     (spice/snn.h:26)                             */
+	uint64_t steps;        /* steps taken so far                                         */
+	uint64_t tile_size;    /* destination neurons per tile (one CTA each)                */
+	uint64_t num_tiles;
+	uint64_t device_bytes; /* device memory held by the net                              */
+} spk_net_info;
+
+/* Message of the last failed call on this host thread ("" if none). */
+char const * spk_last_error( void );
+
+/* Flattened layout: replaces spice::util::layout's constructor and accessors
+ * (spice/util/layout.cpp:51-110, size()/connections()/max_degree() at :111-113).
+ * Writes up to `cap` tuples (src_first, src_last, dst_first, dst_last) to out_ranges and
+ * their probabilities to out_p; *out_count = number of connections. */
+int spk_layout_flatten(
+    spk_layout_desc const * desc,
+    int * out_ranges,
+    float * out_p,
+    int cap,
+    int * out_count,
+    uint64_t * out_size,
+    uint64_t * out_max_degree );
+
+/* Generate the ELL adjacency of `desc` on the device into d_edges
+ * (size * max_degree int32, rows ascending, INT_MAX padded), asynchronously on `stream`.
+ * Replaces spice::cuda::generate_adj_list (spice/cuda/algorithm.h:15). The generator is
+ * counter-based: edge src->dst exists iff Philox(seed; src, j/4, conn, 'GRAP')[j%4] <
+ * floor(p * 2^32) for candidate j = dst - dst_first, truncated at the row width. */
+int spk_generate_adj_list( void * stream, spk_layout_desc const * desc, uint64_t seed, int32_t * d_edges );
+
+/* cuda::snn<Model>(layout, dt, delay) (spice/cuda/snn.h:20-25, spice/cuda/snn.d.cpp:136-165):
+ * allocates the net on `device`, generates the graph from `graph_seed`, initialises
+ * neurons and synapses. `seed` keys the per-(step, neuron) Poisson draws. */
+int spk_net_create(
+    spk_net ** out,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    int device );
+
+/* cuda::snn<Model>(adj, width, dt, delay) (spice/cuda/snn.h:26-32, spice/cuda/snn.d.cpp:167-199):
+ * imports an ELL adjacency (num_neurons x width int32, rows ascending, INT_MAX padded,
+ * width a multiple of 32) from host memory and initialises neurons and synapses. */
+int spk_net_create_from_adj(
+    spk_net ** out,
+    int model,
+    int32_t const * edges,
+    uint64_t num_neurons,
+    uint64_t width,
+    float dt,
+    int delay,
+    uint64_t seed,
+    int device );
+
+/* Import neuron / synapse state from host memory, one array per attribute in the model's
+ * attribute order (float or int32, num_neurons resp. num_synapses entries). With
+ * spk_net_create_from_adj this is the conversion constructor cuda::snn(const snn&)
+ * (spice/cuda/snn.d.cpp:201-221). For brunel_with_plasticity the synapse attributes are
+ * the reference's (W, Zpre, Zpost); Zpre / Zpost must be consistent per neuron. */
+int spk_net_set_neurons( spk_net * net, void * const * attrs );
+int spk_net_set_synapses( spk_net * net, void * const * attrs );
+
+int spk_net_destroy( spk_net * net );
+
+/* snn::step(std::vector<int>* out) (spice/snn.h:22, spice/cuda/snn.d.cpp:224-289).
+ * With out_ids == NULL the step is queued and launched together with later steps (in
+ * windows of up to `delay` steps, identical results). With out_ids != NULL all queued
+ * steps and this one run, and the ids that fired this step are copied out in ascending
+ * order; *out_count receives their number (SPK_ERR_CAPACITY if > cap). */
+int spk_net_step( spk_net * net, int32_t * out_ids, uint64_t cap, uint64_t * out_count );
+
+/* Advance `nsteps` steps: the same as nsteps calls of step(nullptr), launched as
+ * delay-step windows replayed from a CUDA graph. */
+int spk_net_run( spk_net * net, uint64_t nsteps );
+
+/* Advance `nsteps` steps and return their spike raster to host memory: counts[k] = number
+ * of spikes of step k, ids = all spike ids concatenated in step order (ascending within a
+ * step). *out_total = total spikes; SPK_ERR_CAPACITY (state advanced, nothing copied) if
+ * it exceeds ids_cap. */
+int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32_t * ids, uint64_t ids_cap, uint64_t * out_total );
+
+/* The CUDA stream (cudaStream_t) every kernel of this net runs on, for callers that order
+ * their own work or record events against it. Queued steps are launched first. */
+int spk_net_stream( spk_net * net, void ** out_stream );
+
+/* Wait for all queued work; reports device-side errors. */
+int spk_net_sync( spk_net * net );
+
+int spk_net_get_info( spk_net * net, spk_net_info * out );
+
+/* snn::adj() (spice/snn.h:31): the ELL edges (num_neurons * width int32). */
+int spk_net_adj( spk_net * net, int32_t * out, uint64_t cap );
+
+/* snn::neurons() / snn::synapses() (spice/snn.h:32-33) as structure-of-arrays: one host
+ * array per attribute, model attribute order. */
+int spk_net_neurons( spk_net * net, void * const * attrs );
+int spk_net_synapses( spk_net * net, void * const * attrs );
+
+/* Attribute counts of a model's neuron and synapse tuples (as exported above) and, per
+ * attribute, 'f' (float32) or 'i' (int32) in types (neuron attributes, then synapse). */
+int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs, char * types, int types_cap );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPICE_B200_H */

@@ -1,0 +1,315 @@
+"""spice_b200 -- Python binding of the B200 simulation path (libspice_b200.so, C ABI in
+include/spice_b200.h).
+
+Mirrors the reference's interface (spice/snn.h, spice/cuda/snn.h, spice/util/layout.h):
+
+    from spice_b200 import Layout, Snn
+    net = Snn("brunel", Layout([70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)]), dt=1e-4, delay=15)
+    spikes = net.step(out=True)          # snn::step(std::vector<int>*)
+    net.run(100_000)                     # 100k x step(nullptr), CUDA-graph windows
+    edges, width = net.adj()             # snn::adj()
+    V, Twait = net.neurons()             # snn::neurons() as structure of arrays
+
+The compute path is the CUDA library only: importing this module without the built
+library, or constructing a net without a GPU, raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libspice_b200.so")
+
+MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3}
+MODEL_NAMES = {v: k for k, v in MODELS.items()}
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_DEVICE, ERR_CAPACITY = range(6)
+
+
+class SpiceError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class InvalidArgument(SpiceError, ValueError):
+    pass
+
+
+class CapacityError(SpiceError):
+    pass
+
+
+class _LayoutDesc(C.Structure):
+    _fields_ = [
+        ("npops", C.c_int),
+        ("pops", C.POINTER(C.c_uint64)),
+        ("nconn", C.c_int),
+        ("conn_src", C.POINTER(C.c_int)),
+        ("conn_dst", C.POINTER(C.c_int)),
+        ("conn_p", C.POINTER(C.c_float)),
+    ]
+
+
+class NetInfo(C.Structure):
+    _fields_ = [
+        ("model", C.c_int),
+        ("device", C.c_int),
+        ("num_neurons", C.c_uint64),
+        ("num_synapses", C.c_uint64),
+        ("width", C.c_uint64),
+        ("delay", C.c_int),
+        ("dt", C.c_float),
+        ("steps", C.c_uint64),
+        ("tile_size", C.c_uint64),
+        ("num_tiles", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+    ]
+
+
+_lib = None
+
+
+def library():
+    """The loaded libspice_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m spice_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    P, U64, I, F, VP = C.POINTER, C.c_uint64, C.c_int, C.c_float, C.c_void_p
+    sig = {
+        "spk_last_error": (C.c_char_p, []),
+        "spk_layout_flatten": (I, [P(_LayoutDesc), P(I), P(F), I, P(I), P(U64), P(U64)]),
+        "spk_generate_adj_list": (I, [VP, P(_LayoutDesc), U64, VP]),
+        "spk_net_create": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I]),
+        "spk_net_create_from_adj": (I, [P(VP), I, VP, U64, U64, F, I, U64, I]),
+        "spk_net_set_neurons": (I, [VP, P(VP)]),
+        "spk_net_set_synapses": (I, [VP, P(VP)]),
+        "spk_net_destroy": (I, [VP]),
+        "spk_net_step": (I, [VP, VP, U64, P(U64)]),
+        "spk_net_run": (I, [VP, U64]),
+        "spk_net_run_record": (I, [VP, U64, VP, VP, U64, P(U64)]),
+        "spk_net_sync": (I, [VP]),
+        "spk_net_stream": (I, [VP, P(VP)]),
+        "spk_net_get_info": (I, [VP, P(NetInfo)]),
+        "spk_net_adj": (I, [VP, VP, U64]),
+        "spk_net_neurons": (I, [VP, P(VP)]),
+        "spk_net_synapses": (I, [VP, P(VP)]),
+        "spk_model_attrs": (I, [I, P(I), P(I), C.c_char_p, I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code):
+    if code == OK:
+        return
+    msg = library().spk_last_error().decode(errors="replace")
+    if code == ERR_INVALID:
+        raise InvalidArgument(code, msg)
+    if code == ERR_CAPACITY:
+        raise CapacityError(code, msg)
+    raise SpiceError(code, msg)
+
+
+def model_attrs(model):
+    """(neuron attribute dtypes, synapse attribute dtypes) as exported for `model`."""
+    m = MODELS[model] if isinstance(model, str) else int(model)
+    nn, ns = C.c_int(), C.c_int()
+    buf = C.create_string_buffer(32)
+    _check(library().spk_model_attrs(m, C.byref(nn), C.byref(ns), buf, 32))
+    t = buf.value.decode()
+    dt = [np.float32 if c == "f" else np.int32 for c in t]
+    return dt[: nn.value], dt[nn.value: nn.value + ns.value]
+
+
+class Layout:
+    """Populations and (src_pop, dst_pop, p) connections (spice/util/layout.h:30-33).
+    Layout(n, p) is the single-population form."""
+
+    def __init__(self, pops, connections=None):
+        if connections is None:  # Layout(n, p)
+            n, p = pops
+            pops, connections = [int(n)], [(0, 0, float(p))]
+        elif not hasattr(pops, "__len__"):
+            n, p = pops, connections
+            pops, connections = [int(n)], [(0, 0, float(p))]
+        self.pops = [int(x) for x in pops]
+        self.conns = [(int(a), int(b), float(p)) for a, b, p in connections]
+        self._keep = None
+
+    def desc(self):
+        pops = (C.c_uint64 * max(1, len(self.pops)))(*self.pops)
+        src = (C.c_int * max(1, len(self.conns)))(*[c[0] for c in self.conns])
+        dst = (C.c_int * max(1, len(self.conns)))(*[c[1] for c in self.conns])
+        p = (C.c_float * max(1, len(self.conns)))(*[c[2] for c in self.conns])
+        self._keep = (pops, src, dst, p)
+        return _LayoutDesc(len(self.pops), pops, len(self.conns), src, dst, p)
+
+    def _flatten(self):
+        d = self.desc()
+        cap = max(1, len(self.conns))
+        rng = (C.c_int * (4 * cap))()
+        pr = (C.c_float * cap)()
+        cnt, size, width = C.c_int(), C.c_uint64(), C.c_uint64()
+        _check(library().spk_layout_flatten(C.byref(d), rng, pr, cap, C.byref(cnt), C.byref(size), C.byref(width)))
+        conns = [(rng[4 * i], rng[4 * i + 1], rng[4 * i + 2], rng[4 * i + 3], pr[i]) for i in range(cnt.value)]
+        return size.value, conns, width.value
+
+    def size(self):
+        return self._flatten()[0]
+
+    def connections(self):
+        """Flattened (src_first, src_last, dst_first, dst_last, p) tuples, sorted."""
+        return self._flatten()[1]
+
+    def max_degree(self):
+        return self._flatten()[2]
+
+
+def _arr_ptrs(arrays):
+    return (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+
+
+class Snn:
+    """One simulated network on one GPU: the reference's cuda::snn<Model>.
+
+    Snn(model, layout, dt, delay=1, seed=1, graph_seed=1337)   generate the graph on device
+    Snn(model, adj=(edges, width), dt=..., delay=...)           import an ELL adjacency
+    Snn.from_state(model, edges, width, neurons, synapses, ...)  conversion constructor
+    """
+
+    def __init__(self, model, layout=None, dt=1e-4, delay=1, seed=1, graph_seed=1337, device=0, adj=None):
+        lib = library()
+        self.model = model if isinstance(model, str) else MODEL_NAMES[int(model)]
+        m = MODELS[self.model]
+        self._h = C.c_void_p()
+        if adj is not None:
+            edges, width = adj
+            edges = np.ascontiguousarray(edges, dtype=np.int32)
+            width = int(width)
+            n = edges.size // width if width else 0
+            _check(lib.spk_net_create_from_adj(C.byref(self._h), m, edges.ctypes.data, n, width, float(dt), int(delay),
+                                               int(seed), int(device)))
+        else:
+            if layout is None:
+                raise InvalidArgument(ERR_INVALID, "layout or adj required")
+            d = layout.desc()
+            _check(lib.spk_net_create(C.byref(self._h), m, C.byref(d), float(dt), int(delay), int(seed), int(graph_seed),
+                                      int(device)))
+        self._ndt, self._sdt = model_attrs(self.model)
+
+    @classmethod
+    def from_state(cls, model, edges, width, neurons, synapses=None, dt=1e-4, delay=1, seed=1, device=0):
+        """cuda::snn(const snn&) (spice/cuda/snn.d.cpp:201-221): same graph, same state."""
+        net = cls(model, adj=(edges, width), dt=dt, delay=delay, seed=seed, device=device)
+        net.set_neurons(neurons)
+        if synapses is not None and len(net._sdt):
+            net.set_synapses(synapses)
+        return net
+
+    # --- lifecycle ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(library().spk_net_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- stepping -------------------------------------------------------------------
+    def step(self, out=False):
+        """Advance one step. out=True returns the ids that fired (ascending int32)."""
+        lib = library()
+        if not out:
+            _check(lib.spk_net_step(self._h, None, 0, None))
+            return None
+        n = self.num_neurons()
+        buf = np.empty(max(1, n), dtype=np.int32)
+        cnt = C.c_uint64()
+        _check(lib.spk_net_step(self._h, buf.ctypes.data, buf.size, C.byref(cnt)))
+        return buf[: cnt.value].copy()
+
+    def run(self, nsteps):
+        _check(library().spk_net_run(self._h, int(nsteps)))
+
+    def run_record(self, nsteps, cap=None):
+        """Advance nsteps and return (counts[nsteps], ids) of the spike raster."""
+        nsteps = int(nsteps)
+        if cap is None:
+            cap = max(1024, nsteps * max(1, self.num_neurons() // 20))
+        counts = np.empty(max(1, nsteps), dtype=np.uint32)
+        ids = np.empty(max(1, cap), dtype=np.int32)
+        tot = C.c_uint64()
+        _check(library().spk_net_run_record(self._h, nsteps, counts.ctypes.data, ids.ctypes.data, cap, C.byref(tot)))
+        return counts[:nsteps], ids[: tot.value]
+
+    def sync(self):
+        _check(library().spk_net_sync(self._h))
+
+    def stream(self):
+        """cudaStream_t (as int) the net's kernels run on."""
+        v = C.c_void_p()
+        _check(library().spk_net_stream(self._h, C.byref(v)))
+        return v.value or 0
+
+    # --- queries --------------------------------------------------------------------
+    def info(self):
+        i = NetInfo()
+        _check(library().spk_net_get_info(self._h, C.byref(i)))
+        return i
+
+    def num_neurons(self):
+        return self.info().num_neurons
+
+    def num_synapses(self):
+        return self.info().num_synapses
+
+    def dt(self):
+        return self.info().dt
+
+    def delay(self):
+        return self.info().delay
+
+    def adj(self):
+        i = self.info()
+        e = np.empty(max(1, i.num_synapses), dtype=np.int32)
+        _check(library().spk_net_adj(self._h, e.ctypes.data, e.size))
+        return e[: i.num_synapses], i.width
+
+    def neurons(self):
+        n = self.num_neurons()
+        arrs = [np.empty(n, dtype=t) for t in self._ndt]
+        _check(library().spk_net_neurons(self._h, _arr_ptrs(arrs)))
+        return arrs
+
+    def synapses(self):
+        s = self.num_synapses()
+        arrs = [np.empty(s, dtype=t) for t in self._sdt]
+        if arrs:
+            _check(library().spk_net_synapses(self._h, _arr_ptrs(arrs)))
+        return arrs
+
+    def set_neurons(self, arrays):
+        arrs = [np.ascontiguousarray(a, dtype=t) for a, t in zip(arrays, self._ndt)]
+        _check(library().spk_net_set_neurons(self._h, _arr_ptrs(arrs)))
+
+    def set_synapses(self, arrays):
+        arrs = [np.ascontiguousarray(a, dtype=t) for a, t in zip(arrays, self._sdt)]
+        _check(library().spk_net_set_synapses(self._h, _arr_ptrs(arrs)))

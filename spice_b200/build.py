@@ -1,0 +1,77 @@
+"""Build recipe of libspice_b200.so (in-tree, sm_100a).
+
+    python -m spice_b200.build            # builds spice_b200/libspice_b200.so
+
+Flags that matter:
+  -gencode arch=compute_100a,code=sm_100a   B200 only
+  -fmad=false     no contraction of a*b+c into fma: the models' arithmetic stays
+                  operation-for-operation the reference's (explicit fmaf still fuses)
+  no --use_fast_math: IEEE division / expf, denormals kept
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libspice_b200.so")
+SOURCES = [os.path.join(HERE, "csrc", "net.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "plastic.cuh", "device_common.cuh")]
+
+
+def nvcc_path():
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def command(out=LIB, extra=()):
+    return [
+        nvcc_path(),
+        "-gencode", "arch=compute_100a,code=sm_100a",
+        "-lineinfo", "-O3", "-std=c++17",
+        "-fmad=false",
+        "--expt-relaxed-constexpr",
+        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+        "-shared",
+        "-I", os.path.join(ROOT, "include"),
+        "-o", out,
+        *SOURCES,
+        "-lcudart",
+        *extra,
+    ]
+
+
+def _headers():
+    inc = os.path.join(ROOT, "include")
+    out = []
+    for d, _, fs in os.walk(inc):
+        out += [os.path.join(d, f) for f in fs]
+    return out
+
+
+def up_to_date(out=LIB):
+    if not os.path.exists(out):
+        return False
+    t = os.path.getmtime(out)
+    return all(os.path.getmtime(f) <= t for f in DEPS + _headers())
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and up_to_date():
+        return LIB
+    cmd = command(extra=extra)
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    if verbose and (r.stdout or r.stderr):
+        print(r.stdout + r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, extra=[a for a in sys.argv[1:] if a != "--force"])

@@ -1,0 +1,835 @@
+// Host orchestrator of one simulated net (the role of spice::cuda::snn,
+// spice/cuda/snn.d.cpp) and the C ABI declared in include/spice_b200.h.
+//
+// One net = one CUDA stream. Steps requested without output are queued and launched in
+// windows of up to `delay` steps (one kernel launch advances every tile by the whole
+// window); spk_net_run replays a captured CUDA graph of many windows.
+#include "kernels.cuh"
+#include "plastic.cuh"
+
+#include <spice/models/brunel.h>
+#include <spice/models/brunel_with_plasticity.h>
+#include <spice/models/synth.h>
+#include <spice/models/vogels_abbott.h>
+#include <spice/util/layout.h>
+#include <spice_b200.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace
+{
+thread_local std::string g_err;
+
+struct spk_error : std::runtime_error
+{
+	int code;
+	spk_error( int c, std::string const & m )
+	    : std::runtime_error( m )
+	    , code( c )
+	{
+	}
+};
+
+void cuda_check( cudaError_t e, char const * what )
+{
+	if( e == cudaSuccess ) return;
+	if( e == cudaErrorMemoryAllocation )
+	{
+		cudaGetLastError();
+		throw spk_error( SPK_ERR_NOMEM, std::string( what ) + ": " + cudaGetErrorString( e ) );
+	}
+	throw spk_error( SPK_ERR_CUDA, std::string( what ) + ": " + cudaGetErrorString( e ) );
+}
+#define CK( x ) cuda_check( ( x ), #x )
+
+void require( bool ok, char const * msg )
+{
+	if( !ok ) throw spk_error( SPK_ERR_INVALID, msg );
+}
+
+template <typename F>
+int guarded( F && f )
+{
+	try
+	{
+		f();
+		return SPK_OK;
+	}
+	catch( spk_error const & e )
+	{
+		g_err = e.what();
+		return e.code;
+	}
+	catch( std::bad_alloc const & )
+	{
+		g_err = "host allocation failed";
+		return SPK_ERR_NOMEM;
+	}
+	catch( std::exception const & e )
+	{
+		g_err = e.what();
+		return SPK_ERR_INVALID;
+	}
+}
+
+// device allocation owned by the net
+struct dbuf
+{
+	void * p = nullptr;
+	size_t bytes = 0;
+	dbuf() = default;
+	dbuf( dbuf const & ) = delete;
+	dbuf & operator=( dbuf const & ) = delete;
+	~dbuf() { reset(); }
+	void reset()
+	{
+		if( p ) cudaFree( p );
+		p = nullptr;
+		bytes = 0;
+	}
+	void alloc( size_t b )
+	{
+		reset();
+		if( b == 0 ) return;
+		CK( cudaMalloc( &p, b ) );
+		bytes = b;
+	}
+	template <typename T>
+	T * as() const
+	{
+		return static_cast<T *>( p );
+	}
+};
+
+// restores the caller's current device on scope exit
+struct device_guard
+{
+	int prev = -1;
+	explicit device_guard( int dev )
+	{
+		CK( cudaGetDevice( &prev ) );
+		if( prev != dev ) CK( cudaSetDevice( dev ) );
+	}
+	~device_guard()
+	{
+		if( prev >= 0 ) cudaSetDevice( prev );
+	}
+};
+
+struct model_desc
+{
+	int neuron_attrs;
+	int synapse_attrs; // as exported (the reference's tuple)
+	char const * types;
+};
+
+model_desc describe( int model )
+{
+	switch( model )
+	{
+	case SPK_VOGELS_ABBOTT: return { 4, 0, "fffi" };
+	case SPK_BRUNEL: return { 2, 0, "fi" };
+	case SPK_BRUNEL_PLUS: return { 2, 3, "fifff" };
+	case SPK_SYNTH: return { 1, 0, "i" };
+	default: throw spk_error( SPK_ERR_INVALID, "invalid model" );
+	}
+}
+
+spice::util::layout to_layout( spk_layout_desc const * d )
+{
+	require( d != nullptr, "layout descriptor is null" );
+	require( d->npops > 0 && d->pops, "layout must contain at least 1 (non-empty) population" );
+	require( d->nconn >= 0 && ( d->nconn == 0 || ( d->conn_src && d->conn_dst && d->conn_p ) ), "bad connection arrays" );
+	std::vector<size_t> pops( d->pops, d->pops + d->npops );
+	std::vector<std::tuple<size_t, size_t, float>> cs;
+	for( int i = 0; i < d->nconn; i++ )
+	{
+		require( d->conn_src[i] >= 0 && d->conn_dst[i] >= 0, "invalid index in connections matrix" );
+		cs.emplace_back( (size_t)d->conn_src[i], (size_t)d->conn_dst[i], d->conn_p[i] );
+	}
+	return spice::util::layout( pops, cs );
+}
+
+unsigned long long bernoulli_threshold( float p )
+{
+	double const t = std::floor( (double)p * 4294967296.0 );
+	return t >= 4294967296.0 ? 4294967296ull : (unsigned long long)t;
+}
+
+struct tile_cfg
+{
+	int threads, npt, tile, ntiles;
+};
+
+// Tiles of threads * npt destination neurons, one CTA each. Prefer configurations whose
+// CTA count fills the SMs evenly; small nets use few, 128-neuron tiles.
+tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
+{
+	tile_cfg best{ 128, 1, 128, (int)( ( n + 127 ) / 128 ) };
+	if( n <= 128LL * sms ) return best;
+	double best_eff = -1;
+	for( int npt : { 4, 2, 1 } )
+		for( int threads = 64; npt <= max_npt && threads <= 512; threads += 32 )
+		{
+			long long const T = (long long)threads * npt;
+			if( T > max_tile ) continue;
+			long long const ntiles = ( n + T - 1 ) / T;
+			long long const waves = ( ntiles + sms - 1 ) / sms;
+			double const eff = (double)n / ( (double)waves * sms * T );
+			if( eff > best_eff + 1e-9 )
+			{
+				best_eff = eff;
+				best = { threads, npt, (int)T, (int)ntiles };
+			}
+		}
+	return best;
+}
+} // namespace
+
+struct spk_net
+{
+	int model = 0;
+	int device = 0;
+	int sms = 148;
+	cudaStream_t stream = nullptr;
+	long long n = 0, width = 0;
+	int delay = 1;
+	float dt = 0;
+	unsigned long long seed = 0;
+	tile_cfg tc{};
+	std::vector<spk::conn_dev> conns;
+
+	dbuf edges, pivots, ring_ids, ring_cnt, clock, dt_ring, err, conns_dev;
+	dbuf attr[spk::MAX_ATTRS];
+	dbuf gather_ids, gather_cnt, cursor, gather_done, rec_ids, rec_cnt;
+	spk::plastic_state plast; // brunel_with_plasticity only
+
+	unsigned long long steps = 0;   // steps requested so far
+	unsigned long long launched = 0; // steps launched
+	unsigned * host_count = nullptr; // pinned
+
+	cudaGraphExec_t graph = nullptr;
+	int graph_windows = 0, graph_len = 0;
+
+	~spk_net()
+	{
+		if( graph ) cudaGraphExecDestroy( graph );
+		if( host_count ) cudaFreeHost( host_count );
+		if( stream ) cudaStreamDestroy( stream );
+	}
+
+	spk::net_params params() const
+	{
+		spk::net_params p{};
+		p.n = (int)n;
+		p.width = (int)width;
+		p.delay = delay;
+		p.tile = tc.tile;
+		p.ntiles = tc.ntiles;
+		p.ring = 2 * delay;
+		p.seed = seed;
+		p.edges = edges.as<int const>();
+		p.pivots = pivots.as<unsigned const>();
+		for( int i = 0; i < spk::MAX_ATTRS; i++ ) p.attr[i] = attr[i].p;
+		p.ring_ids = ring_ids.as<int>();
+		p.ring_cnt = ring_cnt.as<unsigned>();
+		p.clock = clock.as<spk::clock_state>();
+		p.dt_ring = dt_ring.as<float>();
+		p.err = err.as<int>();
+		return p;
+	}
+
+	size_t device_bytes() const
+	{
+		size_t b = edges.bytes + pivots.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
+		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
+		           rec_cnt.bytes + plast.bytes();
+		for( auto const & a : attr ) b += a.bytes;
+		return b;
+	}
+
+	int window_smem() const
+	{
+		int const classes = model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 );
+		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
+		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
+		if( model == SPK_BRUNEL_PLUS ) b = spk::plastic_window_smem( tc.tile, tc.ntiles, tc.threads );
+		return (int)b;
+	}
+
+	// every kernel a launch can use, with its shared-memory size set (once, outside any
+	// stream capture)
+	template <typename Model, typename F>
+	void with_window_kernel( F && f )
+	{
+		if constexpr( Model::synapse::has_stdp )
+		{
+			switch( tc.npt )
+			{
+			case 4: f( spk::window_plastic<Model, 4> ); break;
+			case 2: f( spk::window_plastic<Model, 2> ); break;
+			default: f( spk::window_plastic<Model, 1> ); break;
+			}
+		}
+		else
+		{
+			switch( tc.npt )
+			{
+			case 4: f( spk::window_counts<Model, 4> ); break;
+			case 2: f( spk::window_counts<Model, 2> ); break;
+			default: f( spk::window_counts<Model, 1> ); break;
+			}
+		}
+	}
+
+	template <typename Model>
+	void configure_model()
+	{
+		int const smem = window_smem();
+		with_window_kernel<Model>( [&]( auto kernel ) {
+			CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) );
+		} );
+	}
+
+	void configure()
+	{
+		switch( model )
+		{
+		case SPK_VOGELS_ABBOTT: configure_model<spice::vogels_abbott>(); break;
+		case SPK_BRUNEL: configure_model<spice::brunel>(); break;
+		case SPK_BRUNEL_PLUS: configure_model<spice::brunel_with_plasticity>(); break;
+		case SPK_SYNTH: configure_model<spice::synth>(); break;
+		}
+	}
+
+	template <typename Model>
+	void launch_window_model( int L )
+	{
+		auto const p = params();
+		int const smem = window_smem();
+		if constexpr( Model::synapse::has_stdp )
+		{
+			auto const q = plast.params();
+			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
+		}
+		else
+			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
+		CK( cudaGetLastError() );
+	}
+
+	void launch_window( int L )
+	{
+		switch( model )
+		{
+		case SPK_VOGELS_ABBOTT: launch_window_model<spice::vogels_abbott>( L ); break;
+		case SPK_BRUNEL: launch_window_model<spice::brunel>( L ); break;
+		case SPK_BRUNEL_PLUS: launch_window_model<spice::brunel_with_plasticity>( L ); break;
+		case SPK_SYNTH: launch_window_model<spice::synth>( L ); break;
+		}
+	}
+
+	int max_window() const { return std::min( delay, spk::MAX_WINDOW ); }
+
+	// launch every queued step
+	void flush()
+	{
+		while( launched < steps )
+		{
+			int const L = (int)std::min<unsigned long long>( steps - launched, (unsigned long long)max_window() );
+			launch_window( L );
+			launched += L;
+		}
+	}
+
+	void check_device_error()
+	{
+		int e = 0;
+		CK( cudaMemcpyAsync( &e, err.p, sizeof( int ), cudaMemcpyDeviceToHost, stream ) );
+		CK( cudaStreamSynchronize( stream ) );
+		if( e ) throw spk_error( SPK_ERR_DEVICE, "device error flag " + std::to_string( e ) );
+	}
+
+	void sync()
+	{
+		flush();
+		check_device_error();
+	}
+
+	// dense ascending spikes of the `count` steps just launched -> ids (device), counts
+	void gather( int count, int * ids, unsigned * counts, unsigned long long cap, long long rec_base )
+	{
+		spk::gather_raster<<<count, 256, 0, stream>>>(
+		    ring_ids.as<int>(),
+		    ring_cnt.as<unsigned>(),
+		    (int)n,
+		    tc.tile,
+		    tc.ntiles,
+		    2 * delay,
+		    clock.as<spk::clock_state>(),
+		    count,
+		    cursor.as<unsigned long long>(),
+		    gather_done.as<unsigned>(),
+		    ids,
+		    counts ? counts + rec_base : nullptr,
+		    cap,
+		    err.as<int>() );
+		CK( cudaGetLastError() );
+	}
+
+	void build_graph_exec( int windows, int len )
+	{
+		if( graph && graph_windows == windows && graph_len == len ) return;
+		if( graph ) cudaGraphExecDestroy( graph );
+		graph = nullptr;
+		cudaGraph_t g;
+		CK( cudaStreamBeginCapture( stream, cudaStreamCaptureModeThreadLocal ) );
+		for( int w = 0; w < windows; w++ ) launch_window( len );
+		CK( cudaStreamEndCapture( stream, &g ) );
+		cudaError_t const e = cudaGraphInstantiate( &graph, g, 0 );
+		cudaGraphDestroy( g );
+		CK( e );
+		graph_windows = windows;
+		graph_len = len;
+	}
+
+	void run( unsigned long long nsteps )
+	{
+		flush();
+		int const len = max_window();
+		unsigned long long const windows = std::min<unsigned long long>( nsteps / len, 512 );
+		if( windows >= 2 )
+		{
+			build_graph_exec( (int)windows, len );
+			unsigned long long const per_graph = windows * len;
+			while( nsteps >= per_graph )
+			{
+				CK( cudaGraphLaunch( graph, stream ) );
+				nsteps -= per_graph;
+				steps += per_graph;
+				launched += per_graph;
+			}
+		}
+		steps += nsteps;
+		flush();
+	}
+};
+
+namespace
+{
+template <typename Model>
+void init_model( spk_net & net )
+{
+	auto const p = net.params();
+	int const blocks = (int)std::min<long long>( 4 * net.sms, ( net.n + 255 ) / 256 );
+	spk::init_neurons<Model><<<std::max( 1, blocks ), 256, 0, net.stream>>>( p );
+	CK( cudaGetLastError() );
+	if constexpr( Model::synapse::has_stdp ) spk::init_plastic<Model>( p, net.plast, net.dt, net.sms, net.stream );
+}
+
+void init_state( spk_net & net )
+{
+	switch( net.model )
+	{
+	case SPK_VOGELS_ABBOTT: init_model<spice::vogels_abbott>( net ); break;
+	case SPK_BRUNEL: init_model<spice::brunel>( net ); break;
+	case SPK_BRUNEL_PLUS: init_model<spice::brunel_with_plasticity>( net ); break;
+	case SPK_SYNTH: init_model<spice::synth>( net ); break;
+	}
+}
+
+// buffers + pivots; edges must be filled before build_pivots is enqueued
+void allocate( spk_net & net, long long n, long long width )
+{
+	require( n > 0 && n <= INT_MAX, "invalid neuron count" );
+	require( width >= 0 && width % 32 == 0, "width must be a multiple of 32" );
+	require( n * std::max<long long>( width, 1 ) < ( 1LL << 40 ), "graph too large" );
+	net.n = n;
+	net.width = width;
+	int dev_sms = 0;
+	CK( cudaDeviceGetAttribute( &dev_sms, cudaDevAttrMultiProcessorCount, net.device ) );
+	net.sms = dev_sms;
+	net.tc = net.model == SPK_BRUNEL_PLUS ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
+	model_desc const md = describe( net.model );
+
+	net.edges.alloc( (size_t)( n * width ) * 4 );
+	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
+	net.ring_ids.alloc( (size_t)2 * net.delay * n * 4 );
+	net.ring_cnt.alloc( (size_t)2 * net.delay * net.tc.ntiles * 4 );
+	net.clock.alloc( sizeof( spk::clock_state ) );
+	net.dt_ring.alloc( spk::DT_RING * 4 );
+	net.err.alloc( 4 );
+	for( int i = 0; i < md.neuron_attrs; i++ ) net.attr[i].alloc( (size_t)n * 4 );
+	net.gather_ids.alloc( (size_t)n * 4 );
+	net.gather_cnt.alloc( 4 );
+	net.cursor.alloc( 8 );
+	net.gather_done.alloc( 4 );
+	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
+	CK( cudaMemsetAsync( net.clock.p, 0, net.clock.bytes, net.stream ) );
+	CK( cudaMemsetAsync( net.err.p, 0, 4, net.stream ) );
+	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
+	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
+	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay );
+	CK( cudaMallocHost( &net.host_count, 16 ) );
+	net.configure();
+}
+
+void enqueue_pivots( spk_net & net )
+{
+	if( net.n == 0 ) return;
+	int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
+	if( net.width > 0 )
+		spk::build_pivots<<<blocks, 256, 0, net.stream>>>(
+		    (int)net.n, (int)net.width, net.tc.tile, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>() );
+	else
+		CK( cudaMemsetAsync( net.pivots.p, 0, net.pivots.bytes, net.stream ) );
+	CK( cudaGetLastError() );
+}
+
+void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned long long seed, int * d_edges, dbuf & conns_dev )
+{
+	std::vector<spk::conn_dev> cs;
+	for( auto const & c : l.connections() )
+		cs.push_back( { std::get<0>( c ), std::get<1>( c ), std::get<2>( c ), std::get<3>( c ), bernoulli_threshold( std::get<4>( c ) ) } );
+	long long const n = (long long)l.size(), w = (long long)l.max_degree();
+	if( n == 0 || w == 0 ) return;
+	conns_dev.alloc( std::max<size_t>( cs.size(), 1 ) * sizeof( spk::conn_dev ) );
+	if( !cs.empty() ) CK( cudaMemcpyAsync( conns_dev.p, cs.data(), cs.size() * sizeof( spk::conn_dev ), cudaMemcpyHostToDevice, s ) );
+	int const blocks = (int)( ( n * 32 + 255 ) / 256 );
+	spk::generate_ell<<<blocks, 256, 0, s>>>( (int)n, (int)w, (int)cs.size(), conns_dev.as<spk::conn_dev>(), seed, d_edges );
+	CK( cudaGetLastError() );
+}
+
+spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int device )
+{
+	describe( model );
+	require( dt > 0.0f, "dt must be > 0" );
+	require( delay >= 1, "delay must be >= 1" );
+	require( model != SPK_BRUNEL_PLUS || delay <= spk::PL_MAX_DELAY, "plastic models support delays up to 63 steps" );
+	int ndev = 0;
+	CK( cudaGetDeviceCount( &ndev ) );
+	require( device >= 0 && device < ndev, "invalid device" );
+	auto net = std::make_unique<spk_net>();
+	net->model = model;
+	net->device = device;
+	net->dt = dt;
+	net->delay = delay;
+	net->seed = seed;
+	CK( cudaStreamCreateWithFlags( &net->stream, cudaStreamNonBlocking ) );
+	return net.release();
+}
+} // namespace
+
+extern "C" {
+char const * spk_last_error( void ) { return g_err.c_str(); }
+
+int spk_layout_flatten(
+    spk_layout_desc const * desc, int * out_ranges, float * out_p, int cap, int * out_count, uint64_t * out_size, uint64_t * out_max_degree )
+{
+	return guarded( [&] {
+		auto const l = to_layout( desc );
+		int i = 0;
+		for( auto const & c : l.connections() )
+		{
+			if( i < cap )
+			{
+				if( out_ranges )
+				{
+					out_ranges[4 * i + 0] = std::get<0>( c );
+					out_ranges[4 * i + 1] = std::get<1>( c );
+					out_ranges[4 * i + 2] = std::get<2>( c );
+					out_ranges[4 * i + 3] = std::get<3>( c );
+				}
+				if( out_p ) out_p[i] = std::get<4>( c );
+			}
+			i++;
+		}
+		if( out_count ) *out_count = i;
+		if( out_size ) *out_size = l.size();
+		if( out_max_degree ) *out_max_degree = l.max_degree();
+	} );
+}
+
+int spk_generate_adj_list( void * stream, spk_layout_desc const * desc, uint64_t seed, int32_t * d_edges )
+{
+	return guarded( [&] {
+		auto const l = to_layout( desc );
+		require( d_edges != nullptr || l.size() * l.max_degree() == 0, "edges pointer is null" );
+		cudaStream_t const s = static_cast<cudaStream_t>( stream );
+		static thread_local dbuf conns; // kept alive until the next call on this thread
+		CK( cudaStreamSynchronize( s ) );
+		enqueue_generate( s, l, seed, d_edges, conns );
+	} );
+}
+
+int spk_net_create( spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device )
+{
+	return guarded( [&] {
+		require( out != nullptr, "out is null" );
+		*out = nullptr;
+		auto const l = to_layout( desc );
+		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
+		device_guard g( device );
+		allocate( *net, (long long)l.size(), (long long)l.max_degree() );
+		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev );
+		enqueue_pivots( *net );
+		init_state( *net );
+		CK( cudaStreamSynchronize( net->stream ) );
+		*out = net.release();
+	} );
+}
+
+int spk_net_create_from_adj(
+    spk_net ** out, int model, int32_t const * edges, uint64_t num_neurons, uint64_t width, float dt, int delay, uint64_t seed, int device )
+{
+	return guarded( [&] {
+		require( out != nullptr, "out is null" );
+		*out = nullptr;
+		require( edges != nullptr || num_neurons * width == 0, "edges is null" );
+		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
+		device_guard g( device );
+		allocate( *net, (long long)num_neurons, (long long)width );
+		// validate rows: ascending, in range, INT_MAX padded
+		for( uint64_t i = 0; i < num_neurons; i++ )
+		{
+			int prev = -1;
+			bool pad = false;
+			for( uint64_t j = 0; j < width; j++ )
+			{
+				int const v = edges[i * width + j];
+				if( v == INT_MAX )
+				{
+					pad = true;
+					continue;
+				}
+				require( !pad, "edges: padding must end a row" );
+				require( v > prev && (uint64_t)v < num_neurons, "edges: rows must be strictly ascending and in range" );
+				prev = v;
+			}
+		}
+		if( num_neurons * width )
+			CK( cudaMemcpyAsync( net->edges.p, edges, num_neurons * width * 4, cudaMemcpyHostToDevice, net->stream ) );
+		enqueue_pivots( *net );
+		init_state( *net );
+		CK( cudaStreamSynchronize( net->stream ) );
+		*out = net.release();
+	} );
+}
+
+int spk_net_set_neurons( spk_net * net, void * const * attrs )
+{
+	return guarded( [&] {
+		require( net && attrs, "null argument" );
+		device_guard g( net->device );
+		net->flush();
+		model_desc const md = describe( net->model );
+		for( int i = 0; i < md.neuron_attrs; i++ )
+			CK( cudaMemcpyAsync( net->attr[i].p, attrs[i], (size_t)net->n * 4, cudaMemcpyHostToDevice, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_set_synapses( spk_net * net, void * const * attrs )
+{
+	return guarded( [&] {
+		require( net && attrs, "null argument" );
+		device_guard g( net->device );
+		net->flush();
+		model_desc const md = describe( net->model );
+		if( md.synapse_attrs == 0 ) return;
+		require( net->steps == 0, "synapse state can only be imported before the first step" );
+		net->plast.import<spice::brunel_with_plasticity>( net->params(), static_cast<float const *>( attrs[0] ),
+		                                                  static_cast<float const *>( attrs[1] ), static_cast<float const *>( attrs[2] ),
+		                                                  net->dt, net->sms, net->stream );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_destroy( spk_net * net )
+{
+	return guarded( [&] {
+		if( !net ) return;
+		{
+			device_guard g( net->device );
+			cudaStreamSynchronize( net->stream );
+		}
+		delete net;
+	} );
+}
+
+int spk_net_step( spk_net * net, int32_t * out_ids, uint64_t cap, uint64_t * out_count )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		device_guard g( net->device );
+		net->steps++;
+		if( !out_ids && !out_count )
+		{
+			if( net->steps - net->launched >= (unsigned long long)net->max_window() ) net->flush();
+			return;
+		}
+		net->flush();
+		CK( cudaMemsetAsync( net->cursor.p, 0, 8, net->stream ) );
+		net->gather( 1, net->gather_ids.as<int>(), net->gather_cnt.as<unsigned>(), (unsigned long long)net->n, 0 );
+		CK( cudaMemcpyAsync( net->host_count, net->gather_cnt.p, 4, cudaMemcpyDeviceToHost, net->stream ) );
+		net->check_device_error();
+		uint64_t const c = net->host_count[0];
+		if( out_count ) *out_count = c;
+		if( !out_ids ) return;
+		if( c > cap ) throw spk_error( SPK_ERR_CAPACITY, "spike buffer too small" );
+		if( c ) CK( cudaMemcpyAsync( out_ids, net->gather_ids.p, c * 4, cudaMemcpyDeviceToHost, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_run( spk_net * net, uint64_t nsteps )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		device_guard g( net->device );
+		net->run( nsteps );
+	} );
+}
+
+int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32_t * ids, uint64_t ids_cap, uint64_t * out_total )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		require( counts != nullptr || nsteps == 0, "counts is null" );
+		device_guard g( net->device );
+		net->flush();
+		if( nsteps == 0 )
+		{
+			if( out_total ) *out_total = 0;
+			return;
+		}
+		if( net->rec_ids.bytes < std::max<uint64_t>( ids_cap, 1 ) * 4 ) net->rec_ids.alloc( std::max<uint64_t>( ids_cap, 1 ) * 4 );
+		if( net->rec_cnt.bytes < nsteps * 4 ) net->rec_cnt.alloc( nsteps * 4 );
+		CK( cudaMemsetAsync( net->cursor.p, 0, 8, net->stream ) );
+		uint64_t done = 0;
+		while( done < nsteps )
+		{
+			int const L = (int)std::min<uint64_t>( nsteps - done, (uint64_t)net->max_window() );
+			net->steps += L;
+			net->launch_window( L );
+			net->launched += L;
+			net->gather( L, net->rec_ids.as<int>(), net->rec_cnt.as<unsigned>(), ids_cap, (long long)done );
+			done += L;
+		}
+		unsigned long long total = 0;
+		CK( cudaMemcpyAsync( net->host_count, net->cursor.p, 8, cudaMemcpyDeviceToHost, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+		std::memcpy( &total, net->host_count, 8 );
+		if( out_total ) *out_total = total;
+		int e = 0;
+		CK( cudaMemcpy( &e, net->err.p, 4, cudaMemcpyDeviceToHost ) );
+		if( e & spk::ERR_OVERFLOW )
+		{
+			CK( cudaMemset( net->err.p, 0, 4 ) );
+			throw spk_error( SPK_ERR_CAPACITY, "spike raster buffer too small" );
+		}
+		if( e ) throw spk_error( SPK_ERR_DEVICE, "device error flag " + std::to_string( e ) );
+		CK( cudaMemcpyAsync( counts, net->rec_cnt.p, nsteps * 4, cudaMemcpyDeviceToHost, net->stream ) );
+		if( total && ids ) CK( cudaMemcpyAsync( ids, net->rec_ids.p, total * 4, cudaMemcpyDeviceToHost, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_stream( spk_net * net, void ** out_stream )
+{
+	return guarded( [&] {
+		require( net && out_stream, "null argument" );
+		device_guard g( net->device );
+		net->flush();
+		*out_stream = net->stream;
+	} );
+}
+
+int spk_net_sync( spk_net * net )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		device_guard g( net->device );
+		net->sync();
+	} );
+}
+
+int spk_net_get_info( spk_net * net, spk_net_info * out )
+{
+	return guarded( [&] {
+		require( net && out, "null argument" );
+		out->model = net->model;
+		out->device = net->device;
+		out->num_neurons = (uint64_t)net->n;
+		out->num_synapses = (uint64_t)( net->n * net->width );
+		out->width = (uint64_t)net->width;
+		out->delay = net->delay;
+		out->dt = net->dt;
+		out->steps = net->steps;
+		out->tile_size = (uint64_t)net->tc.tile;
+		out->num_tiles = (uint64_t)net->tc.ntiles;
+		out->device_bytes = net->device_bytes();
+	} );
+}
+
+int spk_net_adj( spk_net * net, int32_t * out, uint64_t cap )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		uint64_t const need = (uint64_t)( net->n * net->width );
+		if( cap < need ) throw spk_error( SPK_ERR_CAPACITY, "adjacency buffer too small" );
+		device_guard g( net->device );
+		net->sync();
+		if( need ) CK( cudaMemcpyAsync( out, net->edges.p, need * 4, cudaMemcpyDeviceToHost, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_neurons( spk_net * net, void * const * attrs )
+{
+	return guarded( [&] {
+		require( net && attrs, "null argument" );
+		device_guard g( net->device );
+		net->sync();
+		model_desc const md = describe( net->model );
+		for( int i = 0; i < md.neuron_attrs; i++ )
+			CK( cudaMemcpyAsync( attrs[i], net->attr[i].p, (size_t)net->n * 4, cudaMemcpyDeviceToHost, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_synapses( spk_net * net, void * const * attrs )
+{
+	return guarded( [&] {
+		require( net && attrs, "null argument" );
+		device_guard g( net->device );
+		net->sync();
+		model_desc const md = describe( net->model );
+		if( md.synapse_attrs == 0 ) return;
+		CK( net->plast.export_synapses<spice::brunel_with_plasticity>(
+		    net->params(), static_cast<float *>( attrs[0] ), static_cast<float *>( attrs[1] ), static_cast<float *>( attrs[2] ), net->sms,
+		    net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs, char * types, int types_cap )
+{
+	return guarded( [&] {
+		model_desc const md = describe( model );
+		if( num_neuron_attrs ) *num_neuron_attrs = md.neuron_attrs;
+		if( num_synapse_attrs ) *num_synapse_attrs = md.synapse_attrs;
+		if( types && types_cap > 0 )
+		{
+			std::strncpy( types, md.types, (size_t)types_cap - 1 );
+			types[types_cap - 1] = 0;
+		}
+	} );
+}
+}

@@ -1,0 +1,61 @@
+"""The C-ABI library builds for sm_100a, loads, and exports every entry point that
+include/*.h declares (no GPU needed: nothing here launches a kernel)."""
+import glob
+import os
+import re
+
+import pytest
+
+import spice_b200
+from spice_b200 import build as sb_build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(spk_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    sb_build.build()
+    return spice_b200.library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_library_is_sm100a():
+    cmd = sb_build.command()
+    assert "arch=compute_100a,code=sm_100a" in cmd
+    assert "-fmad=false" in cmd and "--use_fast_math" not in cmd
+
+
+def test_errors_without_device_are_reported_not_fatal(lib):
+    # invalid model / invalid layout are rejected before any device work
+    import ctypes as C
+
+    assert lib.spk_model_attrs(9, None, None, None, 0) == spice_b200.ERR_INVALID
+    assert b"invalid model" in lib.spk_last_error()
+    with pytest.raises(spice_b200.InvalidArgument):
+        spice_b200.Layout([10], [(0, 0, 1.5)]).max_degree()
+    nn, ns = spice_b200.model_attrs("brunel_with_plasticity")
+    assert len(nn) == 2 and len(ns) == 3
+
+
+def test_layout_matches_reference_known_answers(lib):
+    L = spice_b200.Layout
+    assert L([10, 20, 30], [(1, 0, 0.5), (2, 1, 0.25), (1, 2, 0.125)]).connections() == [
+        (10, 30, 0, 10, 0.5), (10, 30, 30, 60, 0.125), (30, 60, 10, 30, 0.25)]
+    assert L(100, 1.0).max_degree() == 128
+    assert L(100, 0.0).max_degree() == 0
+    assert L([70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)]).max_degree() == 7328

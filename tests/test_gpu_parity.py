@@ -1,0 +1,231 @@
+"""GPU path vs the oracle (pinned to the reference by test_oracle.py), through the C ABI.
+
+Restates the reference's own parity tests (spice_test/cuda/snn.d.cpp:72-157: init state
+equal at 0.0, 1000-step rasters equal every step, final state close) and extends them to
+Brunel (counter-based Poisson draws make it testable) and Brunel+ (lazy STDP, weights).
+Integer work (graph, rasters, Twait) must be bit-exact; FP32 state is compared bit for bit
+where the arithmetic is the reference's, and within the stated tolerances otherwise.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import spice_b200
+from spice_b200 import Layout, Snn
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+INT_MAX = np.iinfo(np.int32).max
+
+# STDP weights: absolute tolerance against the oracle (weights live in [0, 3e-4]);
+# expf on the device and on the host may differ by an ulp, nothing else differs.
+W_ATOL = 1e-4
+V_RTOL = 1e-5
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def ell(lens, ids, width):
+    e = np.full((len(lens), width), INT_MAX, dtype=np.int32)
+    o = 0
+    for i, k in enumerate(lens):
+        e[i, :k] = ids[o:o + k]
+        o += k
+    return e.reshape(-1)
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+
+
+@pytest.fixture(autouse=True)
+def _dev(gpu, oracle_built):
+    yield
+
+
+# ----------------------------------------------------------------------- graph
+@pytest.mark.parametrize("pops,conns,seed", [
+    ([10, 20, 30], [(0, 0, 0.5), (0, 1, 0.1), (0, 2, 0.5), (1, 0, 1.0), (1, 2, 0.5)], 1),
+    ([100], [(0, 0, 1.0)], 2),
+    ([100], [(0, 0, 0.0)], 2),
+    ([4000], [(0, 0, 0.02)], 3),
+    ([2500, 2500], [(0, 1, 0.1), (1, 1, 0.1)], 4),
+    ([333, 1000, 7], [(0, 1, 0.3), (1, 0, 0.01), (1, 2, 0.9), (2, 2, 1.0), (2, 0, 0.001)], 5),
+])
+def test_generator_bit_exact(pops, conns, seed):
+    net = Snn("brunel", Layout(pops, conns), graph_seed=seed)
+    e, w = net.adj()
+    e2, w2 = oracle.generate(pops, conns, seed, graph="philox")
+    assert w == w2
+    assert np.array_equal(e, e2)
+
+
+def test_generator_large_rows_sampled():
+    # 1e8-synapse Brunel layout, rows sampled against the oracle's random-access rows
+    pops, conns = [22360, 22360], [(0, 1, 0.1), (1, 1, 0.1)]
+    net = Snn("brunel", Layout(pops, conns), graph_seed=77, delay=15)
+    e, w = net.adj()
+    rows = e.reshape(-1, w)
+    rng = np.random.default_rng(0)
+    for r in rng.integers(0, rows.shape[0], 40):
+        assert np.array_equal(rows[r], oracle.philox_row(pops, conns, 77, int(r))), r
+    valid = rows != INT_MAX
+    assert np.all(np.diff(np.where(valid, rows, INT_MAX).astype(np.int64), axis=1)[valid[:, 1:]] > 0)
+    deg = valid.sum(1)
+    assert abs(deg.mean() - 0.1 * 22360) < 5
+
+
+# ----------------------------------------------------------------------- init
+@pytest.mark.parametrize("model", ["vogels_abbott", "brunel", "brunel_with_plasticity"])
+def test_init_state_equals_oracle(model):
+    # spice_test/cuda/snn.d.cpp:72-100: GPU init state == CPU init state at 0.0
+    pops, conns = [100], [(0, 0, 0.1)]
+    net = Snn(model, Layout(pops, conns), dt=1e-4, delay=15)
+    ref = oracle.OracleNet(model, pops, conns, delay=15, graph="philox", graph_seed=1337)
+    assert net.num_neurons() == 100 and net.delay() == 15 and net.dt() == np.float32(1e-4)
+    for a, b in zip(net.neurons(), ref.neurons()):
+        assert bits_equal(a, b)
+    if model == "brunel_with_plasticity":
+        e, _ = net.adj()
+        valid = e != INT_MAX
+        for a, b in zip(net.synapses(), ref.synapses()):
+            assert bits_equal(a[valid], b[valid])
+
+
+# ----------------------------------------------------------------------- dynamics
+def run_parity(model, pops, conns, delay, steps, seed, edges=None, width=None, graph_seed=1337, check_w=False):
+    if edges is None:
+        net = Snn(model, Layout(pops, conns), dt=1e-4, delay=delay, seed=seed, graph_seed=graph_seed)
+        edges, width = net.adj()
+        ref = oracle.OracleNet(model, pops, conns, delay=delay, seed=seed, edges=edges, width=width)
+    else:
+        ref = oracle.OracleNet(model, pops, conns, delay=delay, seed=seed, edges=edges, width=width)
+        net = Snn.from_state(model, edges, width, ref.neurons(), ref.synapses() or None, dt=1e-4, delay=delay, seed=seed)
+    for i in range(steps):
+        a = net.step(out=True)
+        b = ref.step()
+        assert np.array_equal(a, b), f"{model}: raster differs at step {i}"
+    for k, (a, b) in enumerate(zip(net.neurons(), ref.neurons())):
+        assert bits_equal(a, b), f"{model}: neuron attribute {k} differs"
+    if check_w:
+        valid = edges != INT_MAX
+        sa, sb = net.synapses(), ref.synapses()
+        assert np.max(np.abs(sa[0][valid] - sb[0][valid])) <= W_ATOL
+        assert bits_equal(sa[1][valid], sb[1][valid]) and bits_equal(sa[2][valid], sb[2][valid])
+    return net, ref
+
+
+def test_va_step_from_cpu_net():
+    # spice_test/cuda/snn.d.cpp:104-139 (N = 4000, p = 0.02, 1000 steps)
+    ref = oracle.OracleNet("vogels_abbott", [4000], [(0, 0, 0.02)], delay=1, graph="reference", graph_seed=1337)
+    e, w = ref.adj()
+    run_parity("vogels_abbott", [4000], [(0, 0, 0.02)], 1, 1000, 1, edges=e, width=w)
+
+
+def test_va_step_with_delay():
+    # spice_test/cuda/snn.d.cpp:141-157 (delay 8)
+    ref = oracle.OracleNet("vogels_abbott", [4000], [(0, 0, 0.02)], delay=8, graph="reference", graph_seed=1338)
+    e, w = ref.adj()
+    run_parity("vogels_abbott", [4000], [(0, 0, 0.02)], 8, 1000, 1, edges=e, width=w)
+
+
+@pytest.mark.parametrize("name", ["va_n1000_d1", "va_n1000_d8", "brunel_n1000_d15", "brunelp_n600_d15"])
+def test_against_reference_golden(name):
+    g = golden(name)
+    w = int(g["width"])
+    edges = ell(g["lens"], g["ids"], w)
+    pops = [int(x) for x in g["pops"]]
+    conns = [(int(a), int(b), float(np.float32(p))) for a, b, p in g["conns"]]
+    model, delay, seed = str(g["model"]), int(g["delay"]), int(g["seed"])
+    ref = oracle.OracleNet(model, pops, conns, delay=delay, seed=seed, edges=edges, width=w)
+    net = Snn.from_state(model, edges, w, ref.neurons(), ref.synapses() or None, dt=1e-4, delay=delay, seed=seed)
+    counts, spikes = g["counts"], g["spikes"]
+    o = 0
+    for i in range(int(g["steps"])):
+        s = net.step(out=True)
+        assert np.array_equal(s, spikes[o:o + counts[i]]), f"{name}: raster differs at step {i}"
+        o += counts[i]
+    for k, a in enumerate(net.neurons()):
+        assert bits_equal(a, g[f"neuron{k}"]), f"{name}: neuron attribute {k}"
+    if "W" in g:
+        valid = edges != INT_MAX
+        syn = net.synapses()
+        assert np.max(np.abs(syn[0][valid] - g["W"])) <= W_ATOL
+        assert bits_equal(syn[1][valid], g["Zpre"]) and bits_equal(syn[2][valid], g["Zpost"])
+
+
+@pytest.mark.parametrize("delay", [1, 3, 15])
+def test_brunel_generated_graph(delay):
+    run_parity("brunel", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], delay, 1000, 5, graph_seed=21)
+
+
+def test_synth_model():
+    run_parity("synth", [3000], [(0, 0, 0.01)], 4, 300, 9, graph_seed=3)
+
+
+def test_brunel_plus_stdp_active():
+    # small, low-rate net: weights change (not just the first 1000 steps' identity updates)
+    net, ref = run_parity("brunel_with_plasticity", [300, 300], [(0, 1, 0.1), (1, 1, 0.1)], 15, 3000, 7, graph_seed=5,
+                          check_w=True)
+    e, _ = net.adj()
+    w = net.synapses()[0][e != INT_MAX]
+    assert len(np.unique(w)) > 10
+
+
+@pytest.mark.parametrize("delay", [1, 5])
+def test_brunel_plus_short_delays(delay):
+    run_parity("brunel_with_plasticity", [250, 250], [(0, 1, 0.12), (1, 1, 0.12)], delay, 2500, 13, graph_seed=8, check_w=True)
+
+
+def test_fp64_oracle_tolerances():
+    # FP32 GPU against the FP64 oracle: same rasters early on, rates within 1 %
+    pops, conns = [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)]
+    net = Snn("brunel", Layout(pops, conns), delay=15, seed=2, graph_seed=2)
+    e, w = net.adj()
+    ref = oracle.OracleNet("brunel", pops, conns, delay=15, seed=2, edges=e, width=w, precision=64)
+    ca = cb = 0
+    same = 0
+    for i in range(3000):
+        a, b = net.step(out=True), ref.step()
+        ca += len(a)
+        cb += len(b)
+        same += np.array_equal(a, b)
+    assert abs(ca - cb) <= 0.01 * cb
+    assert same >= 1000
+
+
+# ----------------------------------------------------------------------- windows / graphs
+@pytest.mark.parametrize("model,delay", [("brunel", 15), ("vogels_abbott", 1), ("brunel_with_plasticity", 15)])
+def test_run_record_equals_stepping(model, delay):
+    pops, conns = ([3000], [(0, 0, 0.02)]) if model == "vogels_abbott" else ([1500, 1500], [(0, 1, 0.1), (1, 1, 0.1)])
+    a = Snn(model, Layout(pops, conns), delay=delay, seed=4, graph_seed=4)
+    b = Snn(model, Layout(pops, conns), delay=delay, seed=4, graph_seed=4)
+    ref = [a.step(out=True) for _ in range(1234)]
+    counts, ids = b.run_record(1234)
+    assert np.array_equal(counts, [len(x) for x in ref])
+    assert np.array_equal(ids, np.concatenate(ref))
+    # graph replay (run) then stepping stays identical
+    a.run(2100)
+    for _ in range(2100):
+        b.step()
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+    assert np.array_equal(a.step(out=True), b.step(out=True))
+
+
+def test_errors():
+    with pytest.raises(spice_b200.InvalidArgument):
+        Snn("brunel", Layout(10, 0.1), dt=0.0)
+    with pytest.raises(spice_b200.InvalidArgument):
+        Snn("brunel", Layout(10, 0.1), delay=0)
+    with pytest.raises(spice_b200.InvalidArgument):
+        Snn("brunel", adj=(np.array([1, 0] + [INT_MAX] * 30 + [INT_MAX] * 32, np.int32), 32))
+    net = Snn("brunel_with_plasticity", Layout(10, 0.1))
+    net.step()
+    with pytest.raises(spice_b200.InvalidArgument):  # synapse import only before the first step
+        net.set_synapses([np.zeros(net.num_synapses(), np.float32)] * 3)
