@@ -54,6 +54,8 @@ struct brunel_with_plasticity : model
 	struct synapse : ::spice::synapse<float>
 	{
 		static constexpr bool has_stdp = true;
+		// exported as the reference's (W, Zpre, Zpost)
+		using export_tuple_t = std::tuple<float, float, float>;
 
 		template <typename Iter, typename Backend>
 		SPICE_HD static void init( Iter syn, int src, int, snn_info info, Backend & )

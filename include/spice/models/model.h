@@ -98,6 +98,8 @@ template <typename... Ts>
 struct synapse : util::type_list<Ts...>
 {
 	static constexpr bool has_stdp = false;
+	// the tuple synapses() exports (the reference's synapse tuple)
+	using export_tuple_t = std::tuple<Ts...>;
 
 	template <typename Iter, typename Backend>
 	SPICE_HD static void init( Iter, int, int, snn_info, Backend & )

@@ -59,9 +59,14 @@ public:
 			_connections.emplace_back( (int)first[s], (int)first[s + 1], (int)first[d], (int)first[d + 1], std::get<2>( c ) );
 		}
 		_max_degree = estimate_width( _connections );
+		_pops = pops;
+		_pop_connections = conns;
 	}
 
 	std::size_t size() const { return _n; }
+	// the constructor's inputs (connections sorted by (src, dst))
+	std::vector<std::size_t> const & populations() const { return _pops; }
+	std::vector<std::tuple<std::size_t, std::size_t, float>> const & population_connections() const { return _pop_connections; }
 	std::vector<edge> const & connections() const { return _connections; }
 	std::size_t max_degree() const { return _max_degree; }
 
@@ -95,6 +100,8 @@ private:
 	std::size_t _n = 0;
 	std::vector<edge> _connections;
 	std::size_t _max_degree = 0;
+	std::vector<std::size_t> _pops;
+	std::vector<std::tuple<std::size_t, std::size_t, float>> _pop_connections;
 };
 } // namespace util
 } // namespace spice

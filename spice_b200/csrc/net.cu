@@ -15,6 +15,7 @@
 #include <spice_b200.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -168,12 +169,15 @@ struct tile_cfg
 	int threads, npt, tile, ntiles;
 };
 
-// Tiles of threads * npt destination neurons, one CTA each. Prefer configurations whose
-// CTA count fills the SMs evenly; small nets use few, 128-neuron tiles.
+// Tiles of threads * npt destination neurons, one CTA each. Every tile scans every
+// arrival of a step, so fewer, larger tiles do less redundant work: prefer the fewest
+// waves of CTAs over the SMs, then the best fill of the last wave, then larger tiles.
+// Small nets use 128-neuron tiles.
 tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 {
 	tile_cfg best{ 128, 1, 128, (int)( ( n + 127 ) / 128 ) };
 	if( n <= 128LL * sms ) return best;
+	long long best_waves = LLONG_MAX;
 	double best_eff = -1;
 	for( int npt : { 4, 2, 1 } )
 		for( int threads = 64; npt <= max_npt && threads <= 512; threads += 32 )
@@ -183,8 +187,10 @@ tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 			long long const ntiles = ( n + T - 1 ) / T;
 			long long const waves = ( ntiles + sms - 1 ) / sms;
 			double const eff = (double)n / ( (double)waves * sms * T );
-			if( eff > best_eff + 1e-9 )
+			if( waves < best_waves || ( waves == best_waves && eff > best_eff + 1e-6 ) ||
+			    ( waves == best_waves && eff > best_eff - 1e-6 && T > best.tile ) )
 			{
+				best_waves = waves;
 				best_eff = eff;
 				best = { threads, npt, (int)T, (int)ntiles };
 			}

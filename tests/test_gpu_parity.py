@@ -98,6 +98,18 @@ def test_init_state_equals_oracle(model):
 
 
 # ----------------------------------------------------------------------- dynamics
+def check_neurons(model, got, want):
+    """Non-plastic models: bit-identical. Plastic: integer state bit-identical, V within
+    V_RTOL relative (scale: the 20 mV threshold), since weights may differ by an ulp of
+    expf between device and host."""
+    for k, (a, b) in enumerate(zip(got, want)):
+        if model != "brunel_with_plasticity" or a.dtype != np.float32:
+            assert bits_equal(a, b), f"{model}: neuron attribute {k} differs"
+        else:
+            err = np.max(np.abs(a.astype(np.float64) - b) / np.maximum(np.abs(b), 0.02))
+            assert err <= V_RTOL, f"{model}: attribute {k} relative error {err}"
+
+
 def run_parity(model, pops, conns, delay, steps, seed, edges=None, width=None, graph_seed=1337, check_w=False):
     if edges is None:
         net = Snn(model, Layout(pops, conns), dt=1e-4, delay=delay, seed=seed, graph_seed=graph_seed)
@@ -110,8 +122,7 @@ def run_parity(model, pops, conns, delay, steps, seed, edges=None, width=None, g
         a = net.step(out=True)
         b = ref.step()
         assert np.array_equal(a, b), f"{model}: raster differs at step {i}"
-    for k, (a, b) in enumerate(zip(net.neurons(), ref.neurons())):
-        assert bits_equal(a, b), f"{model}: neuron attribute {k} differs"
+    check_neurons(model, net.neurons(), ref.neurons())
     if check_w:
         valid = edges != INT_MAX
         sa, sb = net.synapses(), ref.synapses()
@@ -150,8 +161,7 @@ def test_against_reference_golden(name):
         s = net.step(out=True)
         assert np.array_equal(s, spikes[o:o + counts[i]]), f"{name}: raster differs at step {i}"
         o += counts[i]
-    for k, a in enumerate(net.neurons()):
-        assert bits_equal(a, g[f"neuron{k}"]), f"{name}: neuron attribute {k}"
+    check_neurons(model, net.neurons(), [g[f"neuron{k}"] for k in range(len(net.neurons()))])
     if "W" in g:
         valid = edges != INT_MAX
         syn = net.synapses()
