@@ -87,6 +87,21 @@ int spk_layout_flatten(
  * floor(p * 2^32) for candidate j = dst - dst_first, truncated at the row width. */
 int spk_generate_adj_list( void * stream, spk_layout_desc const * desc, uint64_t seed, int32_t * d_edges );
 
+/* Allocation-free variant of spk_generate_adj_list: the same graph for the same layout and
+ * seed, for callers that must not allocate device memory -- code inside a framework whose
+ * caching allocator owns the device (a raw cudaMalloc takes memory behind the pool's back
+ * and can fail mid-run), or latency-critical loops that cannot pay the device-wide
+ * synchronisation of cudaMalloc/cudaFree. No counterpart in the reference.
+ * The connection table goes to a fixed device array of the library (24 KiB per GPU, held
+ * until the process exits): at most 1024 connections and 1024 populations, larger layouts
+ * are rejected with SPK_ERR_INVALID. d_edges (size * max_degree int32) is the caller's.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current: make it before any stream capture. Every call on a device
+ * shares the one array and leaves its table there; calls whose copies and kernels overlap
+ * on the GPU (different streams) race on it, so order them. The stream must belong to the
+ * current device. */
+int spk_generate_adj_list_static( void * stream, spk_layout_desc const * desc, uint64_t seed, int32_t * d_edges );
+
 /* cuda::snn<Model>(layout, dt, delay) (spice/cuda/snn.h:20-25, spice/cuda/snn.d.cpp:136-165):
  * allocates the net on `device`, generates the graph from `graph_seed`, initialises
  * neurons and synapses. `seed` keys the per-(step, neuron) Poisson draws. */

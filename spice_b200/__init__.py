@@ -84,6 +84,7 @@ def library():
         "spk_last_error": (C.c_char_p, []),
         "spk_layout_flatten": (I, [P(_LayoutDesc), P(I), P(F), I, P(I), P(U64), P(U64)]),
         "spk_generate_adj_list": (I, [VP, P(_LayoutDesc), U64, VP]),
+        "spk_generate_adj_list_static": (I, [VP, P(_LayoutDesc), U64, VP]),
         "spk_net_create": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I]),
         "spk_net_create_from_adj": (I, [P(VP), I, VP, U64, U64, F, I, U64, I]),
         "spk_net_set_neurons": (I, [VP, P(VP)]),

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -838,4 +839,118 @@ int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs,
 		}
 	} );
 }
+}
+
+// ---------------------------------------------------------------------------------------
+// Graph generation without any allocation (spk_generate_adj_list_static).
+//
+// Some callers cannot allocate device memory: code running inside a framework whose
+// caching allocator owns the whole device (a raw cudaMalloc there steals memory the pool
+// has already budgeted and can fail at an arbitrary point), and latency-critical loops
+// that cannot afford the device-wide synchronisation cudaMalloc / cudaFree imply. For
+// them this variant keeps the generator's connection table in a fixed device array of
+// this file instead of a fresh allocation; the host side flattens the layout in stack
+// arrays only.
+// ---------------------------------------------------------------------------------------
+namespace
+{
+constexpr int STATIC_MAX_CONNECTIONS = 1024; // 24 KiB of device memory per GPU, held until exit
+constexpr int STATIC_MAX_POPULATIONS = 1024;
+
+__device__ __align__( 256 ) spk::conn_dev g_static_conns[STATIC_MAX_CONNECTIONS];
+
+// device address of g_static_conns, looked up once per device (host code may not use the
+// symbol itself: on the host it is only a stand-in, not a device address)
+constexpr int MAX_DEVICES = 64;
+void * g_static_conns_ptr[MAX_DEVICES] = {};
+std::mutex g_static_mutex;
+
+void * static_conns_address( int device )
+{
+	require( device >= 0 && device < MAX_DEVICES, "device index out of range" );
+	std::lock_guard<std::mutex> lock( g_static_mutex );
+	if( !g_static_conns_ptr[device] )
+	{
+		void * p = nullptr;
+		CK( cudaGetSymbolAddress( &p, g_static_conns ) );
+		g_static_conns_ptr[device] = p;
+	}
+	return g_static_conns_ptr[device];
+}
+} // namespace
+
+extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc const * d, uint64_t seed, int32_t * d_edges )
+{
+	return guarded( [&] {
+		require( d != nullptr, "layout descriptor is null" );
+		require( d->npops > 0 && d->pops, "layout must contain at least 1 (non-empty) population" );
+		require( d->npops <= STATIC_MAX_POPULATIONS, "spk_generate_adj_list_static: at most 1024 populations" );
+		require( d->nconn >= 0 && d->nconn <= STATIC_MAX_CONNECTIONS, "spk_generate_adj_list_static: at most 1024 connections" );
+		require( d->nconn == 0 || ( d->conn_src && d->conn_dst && d->conn_p ), "bad connection arrays" );
+
+		// the layout, flattened exactly as spice::util::layout does, in stack arrays
+		unsigned long long first[STATIC_MAX_POPULATIONS + 1];
+		first[0] = 0;
+		for( int i = 0; i < d->npops; i++ )
+		{
+			require( d->pops[i] > 0 && d->pops[i] <= (uint64_t)INT_MAX, "invalid population size" );
+			first[i + 1] = first[i] + d->pops[i];
+		}
+		require( first[d->npops] <= (unsigned long long)INT_MAX, "too many neurons" );
+		int order[STATIC_MAX_CONNECTIONS];
+		for( int i = 0; i < d->nconn; i++ )
+		{
+			require( d->conn_src[i] >= 0 && d->conn_src[i] < d->npops && d->conn_dst[i] >= 0 && d->conn_dst[i] < d->npops,
+			         "invalid index in connections matrix" );
+			require( d->conn_p[i] >= 0.0f && d->conn_p[i] <= 1.0f, "invalid connect. prob." );
+			order[i] = i;
+		}
+		auto less = [&]( int a, int b ) {
+			return d->conn_src[a] < d->conn_src[b] || ( d->conn_src[a] == d->conn_src[b] && d->conn_dst[a] < d->conn_dst[b] );
+		};
+		for( int i = 1; i < d->nconn; i++ ) // insertion sort: no temporary buffer
+			for( int j = i; j > 0 && less( order[j], order[j - 1] ); j-- ) std::swap( order[j], order[j - 1] );
+		for( int i = 1; i < d->nconn; i++ )
+			require( less( order[i - 1], order[i] ), "no duplicate edges in connections list allowed" );
+
+		spk::conn_dev table[STATIC_MAX_CONNECTIONS];
+		for( int i = 0; i < d->nconn; i++ )
+		{
+			int const c = order[i], s = d->conn_src[c], t = d->conn_dst[c];
+			table[i] = { (int)first[s], (int)first[s + 1], (int)first[t], (int)first[t + 1], bernoulli_threshold( d->conn_p[c] ) };
+		}
+		// width: mean + 3 sigma of the busiest source population, rounded up to 32
+		size_t widest = 0;
+		double mean = 0.0, var = 0.0;
+		int src = d->nconn ? table[0].src_first : 0;
+		for( int i = 0; i < d->nconn; i++ )
+		{
+			if( table[i].src_first != src )
+			{
+				widest = std::max( widest, static_cast<size_t>( mean + 3 * std::sqrt( var ) ) );
+				src = table[i].src_first;
+				mean = var = 0.0;
+			}
+			double const range = static_cast<double>( table[i].dst_last - table[i].dst_first );
+			float const p = d->conn_p[order[i]];
+			mean += range * p;
+			var += range * p * ( 1.0 - p );
+		}
+		widest = std::max( widest, static_cast<size_t>( mean + 3 * std::sqrt( var ) ) );
+		long long const n = (long long)first[d->npops], w = (long long)( ( widest + 31 ) / 32 * 32 );
+		require( d_edges != nullptr || n * w == 0, "edges pointer is null" );
+		if( n * w == 0 ) return;
+
+		int device = 0;
+		CK( cudaGetDevice( &device ) );
+		void * conns = static_conns_address( device );
+		cudaStream_t const s = static_cast<cudaStream_t>( stream );
+		if( d->nconn )
+			CK( cudaMemcpyAsync( conns, table, (size_t)d->nconn * sizeof( spk::conn_dev ), cudaMemcpyHostToDevice, s ) );
+		int const blocks = (int)( ( n * 32 + 255 ) / 256 );
+		spk::generate_ell<<<blocks, 256, 0, s>>>( (int)n, (int)w, d->nconn, static_cast<spk::conn_dev const *>( conns ), seed, d_edges );
+		CK( cudaGetLastError() );
+		// cudaMemcpyAsync from pageable memory returns once the source has been staged, so
+		// the stack table may go out of scope while the copy and the kernel are in flight
+	} );
 }
