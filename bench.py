@@ -41,7 +41,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
-    return ap.parse_args()
+    ap.add_argument("--syn", type=float, default=1e9,
+                    help="total synapses of the Brunel net (the benchmark is 1e9; smaller sizes serve profiling)")
+    args = ap.parse_args()
+    if args.syn != 1e9:
+        # samples/main.cpp:1283,1395: N = sqrt(syn / 0.05), two populations of N / 2
+        half = int((args.syn / 0.05) ** 0.5) // 2
+        POPS[:] = [half, half]
+    return args
 
 
 def dist_init(n):
@@ -262,7 +269,7 @@ def run_ours(args, rank, world):
         line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "brunel_1e9", "neurons": n, "synapses": 1e9, "ell_width": info.width,
+                "config": {"workload": f"brunel_{args.syn:.0e}".replace("+0", ""), "neurons": n, "synapses": args.syn, "ell_width": info.width,
                            "dt": DT, "delay": DELAY, "model": "brunel", "sim_steps_per_bench_step": S,
                            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (4.15 GB synapse table)",
                            "tiles": info.num_tiles, "tile_size": info.tile_size, "setup_s": setup_s,

@@ -17,7 +17,10 @@
 //    The kernels then count arrivals per (destination, class) with integer shared-memory
 //    atomics and replay them as class_source(0) x count0, class_source(1) x count1, ...
 //    through the model's own receive(): the same floating-point additions, in the same
-//    order, as the reference's ascending-source delivery.
+//    order, as the reference's ascending-source delivery. The replay calls receive() once
+//    per class with a backend whose atomic_add(attr, value) adds `value` count times in
+//    sequence, so a model with input classes must change state in receive() only through
+//    one atomic_add whose value does not depend on the attribute it adds to.
 //
 //  * pair STDP with per-neuron traces (plastic models). See brunel_with_plasticity.h.
 #pragma once

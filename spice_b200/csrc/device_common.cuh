@@ -169,6 +169,29 @@ struct device_backend
 	__device__ __forceinline__ static float pow( float x, float y ) { return powf( x, y ); }
 };
 
+// Backend for replaying `times` identical arrivals through one receive() call: its
+// atomic_add performs the `times` additions one after another -- the same sequence of
+// roundings as `times` separate calls -- while the rest of receive() (conditions,
+// constants) runs once. Valid for receive() functions that change state only through
+// one atomic_add whose value does not depend on the attribute it adds to (the input-class
+// contract of include/spice/models/model.h).
+struct repeat_backend : device_backend
+{
+	unsigned times;
+	__device__ __forceinline__ repeat_backend( uint64_t seed, uint32_t neuron_, uint32_t step_, unsigned times_ )
+	    : device_backend( seed, neuron_, step_ )
+	    , times( times_ )
+	{
+	}
+	template <typename T>
+	__device__ __forceinline__ void atomic_add( T & var, T val ) const
+	{
+		T v = var;
+		for( unsigned r = 0; r < times; r++ ) v += val;
+		var = v;
+	}
+};
+
 // Kahan-compensated clock (spice/snn.cpp:38-44, spice/util/numeric.h:9-33): the dt a step
 // hands to the models is the compensated delta.
 struct clock_state

@@ -244,14 +244,14 @@ __device__ __forceinline__ void deliver_counts(
 // -> update -> ordered spike compaction, L steps per launch.
 // ------------------------------------------------------------------------------------
 template <typename Model, int NPT>
-__global__ void __launch_bounds__( 512 ) window_counts( net_params p, int L, float dt )
+__global__ void __launch_bounds__( 512, 1 ) window_counts( net_params p, int L, float dt )
 {
 	using N = typename Model::neuron;
 	using Tup = typename N::template apply<reg_tuple>;
 	constexpr int C = N::input_classes;
 	static_assert( C >= 1, "window_counts needs a model with input classes" );
 
-	extern __shared__ __align__( 16 ) unsigned char smem[];
+	extern __shared__ __align__( 128 ) unsigned char smem[];
 	__shared__ int scratch[33];
 	__shared__ float s_dt[MAX_WINDOW];
 	__shared__ long long s_t0;
@@ -302,8 +302,11 @@ __global__ void __launch_bounds__( 512 ) window_counts( net_params p, int L, flo
 					for( int c = 0; c < C; c++ )
 					{
 						unsigned const m = cnt[c * T + NPT * tid + q];
-						int const s = N::class_source( c, info );
-						for( unsigned r = 0; r < m; r++ ) N::receive( s, it, null_syn_iter{}, info, bak );
+						if( m )
+						{
+							repeat_backend rb( p.seed, (uint32_t)i, (uint32_t)t, m );
+							N::receive( N::class_source( c, info ), it, null_syn_iter{}, info, rb );
+						}
 					}
 				if( N::update( it, s_dt[k], info, bak ) ) fired |= 1u << q;
 			}

@@ -191,13 +191,13 @@ __device__ __forceinline__ void window_trace( float zrf, int rf_off, long long t
 }
 
 template <typename Model, int NPT>
-__global__ void __launch_bounds__( 512 ) window_plastic( net_params p, plastic_params q, int L, float dt )
+__global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plastic_params q, int L, float dt )
 {
 	using N = typename Model::neuron;
 	using Syn = typename Model::synapse;
 	using Tup = typename N::template apply<reg_tuple>;
 
-	extern __shared__ __align__( 16 ) unsigned char smem[];
+	extern __shared__ __align__( 128 ) unsigned char smem[];
 	__shared__ int scratch[33];
 	__shared__ float s_dt[2 * MAX_WINDOW];
 	__shared__ long long s_t0;
