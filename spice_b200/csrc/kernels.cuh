@@ -4,15 +4,15 @@
 //   edges    int32 [n x width]      ELL rows, ascending, INT_MAX padded (the reference's
 //                                   adjacency format, spice/util/adj_list.cpp:28-46)
 //   pivots   uint32 [n x (ntiles+1)] pivots[src][j] = first position in row src whose
-//                                   target is >= j * tile (row slice of tile j)
+//                                   target is >= tile_first[j] (row slice of tile j)
 //   attr[k]  neuron attribute k, structure of arrays
 //   ring_ids int32 [2*delay x n]    spike queue: slot s holds, per tile j, the ids that
 //                                   fired in tile j at a step t with t % (2 delay) == s,
 //                                   ascending, in the segment [j*tile, j*tile + count)
 //   ring_cnt uint32 [2*delay x ntiles]
 //
-// Execution: the destination neurons are cut into `ntiles` tiles of `tile` neurons, one
-// CTA per tile. A spike fired at step t reaches its targets at step t + delay, so all the
+// Execution: the destination neurons are cut into `ntiles` contiguous tiles
+// [tile_first[j], tile_first[j + 1]), one CTA per tile. A spike fired at step t reaches its targets at step t + delay, so all the
 // arrivals of the steps [t0, t0 + L) with L <= delay were fired before t0: one launch
 // advances every tile by L steps with no grid-wide synchronisation inside the launch
 // (the kernel boundary is the only barrier, once per window). The ring has 2*delay slots
@@ -55,6 +55,7 @@ struct net_params
 	unsigned long long seed;
 	int const * edges;
 	unsigned const * pivots;
+	int const * tile_first; // [ntiles + 1] first neuron of every tile
 	void * attr[MAX_ATTRS];
 	int * ring_ids;
 	unsigned * ring_cnt;
@@ -216,7 +217,7 @@ __device__ __forceinline__ void deliver_counts(
 				else
 					hi = mid;
 			}
-			int const src = p.ring_ids[(long long)slot_in * p.n + (long long)lo * p.tile + ( g - pref[lo] )];
+			int const src = p.ring_ids[(long long)slot_in * p.n + __ldg( p.tile_first + lo ) + ( g - pref[lo] )];
 			unsigned const * pv = p.pivots + (long long)src * ( p.ntiles + 1 ) + tile;
 			sb[x] = make_int4( src, (int)__ldg( pv ), (int)__ldg( pv + 1 ), Neuron::input_class( src, info ) );
 		}
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__( 512, 1 ) window_counts( net_params p, int L, 
 	int4 * sb = reinterpret_cast<int4 *>( smem + ( ( ( C * T + p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
 
 	int const tile = blockIdx.x, tid = threadIdx.x;
-	int const d0 = tile * T, d1 = min( p.n, d0 + T );
+	int const d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 );
 	snn_info const info{ p.n };
 
 	window_clock_begin( p, L, dt, s_dt, &s_t0, &s_c, &s_sum );
@@ -380,8 +381,8 @@ __global__ void __launch_bounds__( 256 ) generate_ell( int n, int width, int nco
 	for( int e = a + 4 * lane; e < width; e += 128 ) *reinterpret_cast<int4 *>( row + e ) = pad;
 }
 
-// pivots[src][j] = lower_bound(row src, j * tile) for j = 0..ntiles; one warp per row.
-__global__ void __launch_bounds__( 256 ) build_pivots( int n, int width, int tile, int ntiles, int const * edges, unsigned * pivots )
+// pivots[src][j] = lower_bound(row src, tile_first[j]) for j = 0..ntiles; one warp per row.
+__global__ void __launch_bounds__( 256 ) build_pivots( int n, int width, int const * tile_first, int ntiles, int const * edges, unsigned * pivots )
 {
 	int const warp = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5, lane = threadIdx.x & 31;
 	if( warp >= n ) return;
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__( 256 ) build_pivots( int n, int width, int til
 	unsigned * out = pivots + (long long)warp * ( ntiles + 1 );
 	for( int j = lane; j <= ntiles; j += 32 )
 	{
-		long long const key = (long long)j * tile;
+		long long const key = tile_first[j];
 		int lo = 0, hi = width; // first position with row[pos] >= key
 		while( lo < hi )
 		{
@@ -427,7 +428,7 @@ __global__ void gather_raster(
     int const * ring_ids,
     unsigned const * ring_cnt,
     int n,
-    int tile,
+    int const * tile_first,
     int ntiles,
     int ring,
     clock_state const * clock,
@@ -478,7 +479,7 @@ __global__ void gather_raster(
 		for( int r = 0; r < c; r++ )
 		{
 			if( (unsigned long long)( dst + r ) < out_cap )
-				out_ids[dst + r] = ring_ids[(long long)slot * n + (long long)i * tile + r];
+				out_ids[dst + r] = ring_ids[(long long)slot * n + tile_first[i] + r];
 			else
 				atomicOr( err, ERR_OVERFLOW );
 		}

@@ -5,6 +5,7 @@
 // windows of up to `delay` steps (one kernel launch advances every tile by the whole
 // window); spk_net_run replays a captured CUDA graph of many windows.
 #include "kernels.cuh"
+#include "flat.cuh"
 #include "plastic.cuh"
 
 #include <spice/models/brunel.h>
@@ -17,6 +18,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -213,7 +215,8 @@ struct spk_net
 	tile_cfg tc{};
 	std::vector<spk::conn_dev> conns;
 
-	dbuf edges, pivots, ring_ids, ring_cnt, clock, dt_ring, err, conns_dev;
+	dbuf edges, pivots, tile_first, ring_ids, ring_cnt, clock, dt_ring, err, conns_dev;
+	std::vector<int> tile_first_host; // [ntiles + 1]
 	dbuf attr[spk::MAX_ATTRS];
 	dbuf gather_ids, gather_cnt, cursor, gather_done, rec_ids, rec_cnt;
 	spk::plastic_state plast; // brunel_with_plasticity only
@@ -224,6 +227,10 @@ struct spk_net
 
 	cudaGraphExec_t graph = nullptr;
 	int graph_windows = 0, graph_len = 0;
+	// window kernel of non-plastic models: window_flat (staged arrival table, work-balanced
+	// tiles, neuron state in shared memory) where it applies, else window_counts
+	bool flat = false;
+	int flat_tmax = 0; // the largest tile of the flat tiling
 
 	~spk_net()
 	{
@@ -244,6 +251,7 @@ struct spk_net
 		p.seed = seed;
 		p.edges = edges.as<int const>();
 		p.pivots = pivots.as<unsigned const>();
+		p.tile_first = tile_first.as<int const>();
 		for( int i = 0; i < spk::MAX_ATTRS; i++ ) p.attr[i] = attr[i].p;
 		p.ring_ids = ring_ids.as<int>();
 		p.ring_cnt = ring_cnt.as<unsigned>();
@@ -255,16 +263,20 @@ struct spk_net
 
 	size_t device_bytes() const
 	{
-		size_t b = edges.bytes + pivots.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
+		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
 		           rec_cnt.bytes + plast.bytes();
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
 
+	int classes() const { return model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 ); }
+	int neuron_attrs() const { return model == SPK_VOGELS_ABBOTT ? 4 : ( model == SPK_SYNTH ? 1 : 2 ); }
+
 	int window_smem() const
 	{
-		int const classes = model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 );
+		if( flat ) return (int)spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax );
+		int const classes = this->classes();
 		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
 		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
 		if( model == SPK_BRUNEL_PLUS ) b = spk::plastic_window_smem( tc.tile, tc.ntiles, tc.threads );
@@ -300,6 +312,12 @@ struct spk_net
 	void configure_model()
 	{
 		int const smem = window_smem();
+		if constexpr( Model::neuron::input_classes > 0 )
+			if( flat )
+			{
+				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) );
+				return;
+			}
 		with_window_kernel<Model>( [&]( auto kernel ) {
 			CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) );
 		} );
@@ -326,6 +344,8 @@ struct spk_net
 			auto const q = plast.params();
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
 		}
+		else if( flat )
+			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, flat_tmax );
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
 		CK( cudaGetLastError() );
@@ -376,7 +396,7 @@ struct spk_net
 		    ring_ids.as<int>(),
 		    ring_cnt.as<unsigned>(),
 		    (int)n,
-		    tc.tile,
+		    tile_first.as<int>(),
 		    tc.ntiles,
 		    2 * delay,
 		    clock.as<spk::clock_state>(),
@@ -451,8 +471,121 @@ void init_state( spk_net & net )
 	}
 }
 
+// Work per neuron, piecewise constant: neurons [start, next start) cost `cost` each.
+struct cost_segment
+{
+	long long start;
+	double cost;
+};
+
+// one neuron update against one delivered synapse, for tile balancing
+constexpr double UPDATE_COST = 32.0;
+
+// expected in-degree of every neuron of a layout (constant over stretches of populations)
+std::vector<cost_segment> layout_costs( spice::util::layout const & l )
+{
+	std::vector<long long> cuts{ 0, (long long)l.size() };
+	for( auto const & c : l.connections() )
+	{
+		cuts.push_back( std::get<2>( c ) );
+		cuts.push_back( std::get<3>( c ) );
+	}
+	std::sort( cuts.begin(), cuts.end() );
+	cuts.erase( std::unique( cuts.begin(), cuts.end() ), cuts.end() );
+	std::vector<cost_segment> segs;
+	for( size_t i = 0; i + 1 < cuts.size(); i++ )
+	{
+		double in = 0;
+		for( auto const & c : l.connections() )
+			if( std::get<2>( c ) <= cuts[i] && cuts[i] < std::get<3>( c ) ) in += (double)( std::get<1>( c ) - std::get<0>( c ) ) * std::get<4>( c );
+		segs.push_back( { cuts[i], UPDATE_COST + in } );
+	}
+	return segs;
+}
+
+// exact in-degree of every neuron of an imported ELL graph (edges already validated)
+std::vector<cost_segment> adjacency_costs( int const * edges, long long n, long long width )
+{
+	std::vector<int> in( n, 0 );
+	for( long long e = 0; e < n * width; e++ )
+		if( edges[e] != INT_MAX ) in[edges[e]]++;
+	std::vector<cost_segment> segs;
+	for( long long i = 0; i < n; i++ )
+		if( i == 0 || in[i] != in[i - 1] ) segs.push_back( { i, UPDATE_COST + in[i] } );
+	return segs;
+}
+
+// Cut [0, n) into contiguous tiles of about equal work, at most tmax neurons each,
+// aiming at no more tiles than SMs (every tile scans every arrival of a step).
+std::vector<int> balanced_tiles( std::vector<cost_segment> const & segs, long long n, int sms, int tmax )
+{
+	auto seg_end = [&]( size_t i ) { return i + 1 < segs.size() ? segs[i + 1].start : n; };
+	double total = 0;
+	for( size_t i = 0; i < segs.size(); i++ ) total += ( seg_end( i ) - segs[i].start ) * segs[i].cost;
+	auto cut = [&]( double target ) {
+		std::vector<int> first{ 0 };
+		long long start = 0;
+		double acc = 0;
+		for( size_t i = 0; i < segs.size(); i++ )
+		{
+			double const c = std::max( segs[i].cost, 1e-9 );
+			long long pos = segs[i].start;
+			long long const e = seg_end( i );
+			while( pos < e )
+			{
+				long long const room = tmax - ( pos - start );
+				long long fit = (long long)std::floor( ( target - acc ) / c );
+				if( pos == start ) fit = std::max( fit, 1LL );
+				long long const take = std::min( { e - pos, room, std::max( fit, 0LL ) } );
+				if( take <= 0 ) // this tile is full: the next one starts here
+				{
+					first.push_back( (int)pos );
+					start = pos;
+					acc = 0;
+					continue;
+				}
+				pos += take;
+				acc += take * c;
+				if( ( acc >= target * ( 1 - 1e-12 ) || pos - start >= tmax ) && pos < n )
+				{
+					first.push_back( (int)pos );
+					start = pos;
+					acc = 0;
+				}
+			}
+		}
+		if( first.back() != (int)n ) first.push_back( (int)n );
+		return first;
+	};
+	// small nets: at least 256 neurons' worth of work per tile
+	double target = std::max( total / sms, 256.0 * total / std::max<long long>( n, 1 ) );
+	std::vector<int> best = cut( target );
+	for( int it = 0; it < 400 && (int)best.size() - 1 > sms; it++ )
+	{
+		target *= 1.01;
+		best = cut( target );
+	}
+	return best;
+}
+
+std::vector<int> uniform_tiles( long long n, int tile )
+{
+	std::vector<int> f;
+	for( long long d = 0; d < n; d += tile ) f.push_back( (int)d );
+	f.push_back( (int)n );
+	return f;
+}
+
+void set_tiles( spk_net & net, std::vector<int> const & first )
+{
+	net.tile_first_host = first;
+	net.tc.ntiles = (int)first.size() - 1;
+	net.tile_first.alloc( first.size() * 4 );
+	CK( cudaMemcpy( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice ) );
+}
+
 // buffers + pivots; edges must be filled before build_pivots is enqueued
-void allocate( spk_net & net, long long n, long long width )
+void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs )
 {
 	require( n > 0 && n <= INT_MAX, "invalid neuron count" );
 	require( width >= 0 && width % 32 == 0, "width must be a multiple of 32" );
@@ -465,6 +598,34 @@ void allocate( spk_net & net, long long n, long long width )
 	net.tc = net.model == SPK_BRUNEL_PLUS ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
 	model_desc const md = describe( net.model );
 
+	// window kernel and tiling: window_flat with work-balanced tiles (SPK_TILES=uniform keeps
+	// equal tiles, SPK_KERNEL=direct selects window_counts)
+	net.flat = false;
+	char const * kern = getenv( "SPK_KERNEL" );
+	if( net.model != SPK_BRUNEL_PLUS && width < spk::FLAT_MAX_WIDTH && !( kern && !strcmp( kern, "direct" ) ) )
+	{
+		int optin = 0;
+		CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net.device ) );
+		long long const room = (long long)optin - 4096 - (long long)spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), 0 );
+		long long const per_neuron8 = 8LL * 4 * ( net.classes() + net.neuron_attrs() ) + 1; // bytes x 8 per neuron
+		int const tmax = (int)std::min<long long>( spk::FLAT_MAX_TILE, room > 0 ? room * 8 / per_neuron8 / 32 * 32 : 0 );
+		if( tmax >= 128 )
+		{
+			char const * tiling = getenv( "SPK_TILES" );
+			std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
+			                                                                       : balanced_tiles( segs, n, dev_sms, tmax );
+			if( (int)first.size() - 1 < spk::FLAT_SCRATCH )
+			{
+				int span = 0;
+				for( size_t i = 0; i + 1 < first.size(); i++ ) span = std::max( span, first[i + 1] - first[i] );
+				net.flat = true;
+				net.flat_tmax = ( span + 31 ) / 32 * 32;
+				net.tc = { 512, 1, net.flat_tmax, (int)first.size() - 1 };
+				set_tiles( net, first );
+			}
+		}
+	}
+	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.edges.alloc( (size_t)( n * width ) * 4 );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
 	net.ring_ids.alloc( (size_t)2 * net.delay * n * 4 );
@@ -493,7 +654,7 @@ void enqueue_pivots( spk_net & net )
 	int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
 	if( net.width > 0 )
 		spk::build_pivots<<<blocks, 256, 0, net.stream>>>(
-		    (int)net.n, (int)net.width, net.tc.tile, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>() );
+		    (int)net.n, (int)net.width, net.tile_first.as<int>(), net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>() );
 	else
 		CK( cudaMemsetAsync( net.pivots.p, 0, net.pivots.bytes, net.stream ) );
 	CK( cudaGetLastError() );
@@ -583,7 +744,7 @@ int spk_net_create( spk_net ** out, int model, spk_layout_desc const * desc, flo
 		auto const l = to_layout( desc );
 		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
 		device_guard g( device );
-		allocate( *net, (long long)l.size(), (long long)l.max_degree() );
+		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ) );
 		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev );
 		enqueue_pivots( *net );
 		init_state( *net );
@@ -601,7 +762,6 @@ int spk_net_create_from_adj(
 		require( edges != nullptr || num_neurons * width == 0, "edges is null" );
 		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
 		device_guard g( device );
-		allocate( *net, (long long)num_neurons, (long long)width );
 		// validate rows: ascending, in range, INT_MAX padded
 		for( uint64_t i = 0; i < num_neurons; i++ )
 		{
@@ -620,6 +780,7 @@ int spk_net_create_from_adj(
 				prev = v;
 			}
 		}
+		allocate( *net, (long long)num_neurons, (long long)width, adjacency_costs( edges, (long long)num_neurons, (long long)width ) );
 		if( num_neurons * width )
 			CK( cudaMemcpyAsync( net->edges.p, edges, num_neurons * width * 4, cudaMemcpyHostToDevice, net->stream ) );
 		enqueue_pivots( *net );

@@ -157,7 +157,7 @@ __device__ __forceinline__ void stage_spikes( net_params const & p, plastic_para
 	{
 		int const g = b0 + x;
 		int const st = find_tile( pref, p.ntiles, g );
-		long long const pos = (long long)slot * p.n + (long long)st * p.tile + ( g - pref[st] );
+		long long const pos = (long long)slot * p.n + __ldg( p.tile_first + st ) + ( g - pref[st] );
 		int const src = p.ring_ids[pos];
 		int4 const meta = q.ring_meta[pos];
 		unsigned const * pv = p.pivots + (long long)src * ( p.ntiles + 1 ) + tile;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void stage_flushes( net_params const & p, plastic_par
 	{
 		int const g = b0 + x;
 		int const st = find_tile( pref, p.ntiles, g );
-		int4 const f = q.flush_ring[(long long)slot * p.n + (long long)st * p.tile + ( g - pref[st] )];
+		int4 const f = q.flush_ring[(long long)slot * p.n + __ldg( p.tile_first + st ) + ( g - pref[st] )];
 		unsigned const * pv = p.pivots + (long long)f.x * ( p.ntiles + 1 ) + tile;
 		sb[x] = { f.x, (int)__ldg( pv ), (int)__ldg( pv + 1 ), f.y, __int_as_float( f.z ), 0.0f };
 	}
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 
 	int const T = p.tile, tid = threadIdx.x;
 	int const warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-	int const tile = blockIdx.x, d0 = tile * T, d1 = min( p.n, d0 + T ), span = d1 - d0;
+	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	snn_info const info{ p.n };
 
 	// shared memory carve-up (sizes: see plastic_window_smem)

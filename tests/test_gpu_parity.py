@@ -239,3 +239,26 @@ def test_errors():
     net.step()
     with pytest.raises(spice_b200.InvalidArgument):  # synapse import only before the first step
         net.set_synapses([np.zeros(net.num_synapses(), np.float32)] * 3)
+
+
+# ----------------------------------------------------------------------- window kernel paths
+@pytest.mark.parametrize("n,delay,steps", [
+    (400_000, 15, 60),     # ~2000 arrivals per step: window tables split into segments
+    (1_700_000, 4, 24),    # > 8192 arrivals in one step: the direct path inside window_flat
+])
+def test_flat_kernel_matches_direct_kernel(n, delay, steps):
+    """window_flat (staged table, balanced tiles) against window_counts, itself checked
+    against the oracle above, on nets too large for the oracle to step quickly."""
+    layout = Layout(n, 16.0 / n)
+    a = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
+    os.environ["SPK_KERNEL"] = "direct"
+    try:
+        b = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
+    finally:
+        del os.environ["SPK_KERNEL"]
+    assert a.info().num_tiles != b.info().num_tiles or a.info().tile_size != b.info().tile_size
+    ca, ia = a.run_record(steps, cap=n * steps // 50)
+    cb, ib = b.run_record(steps, cap=n * steps // 50)
+    assert ca.max() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert np.array_equal(x, y)
