@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspice_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "net.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "plastic.cuh", "device_common.cuh")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "plastic.cuh", "flat.cuh", "device_common.cuh")]
 
 
 def nvcc_path():

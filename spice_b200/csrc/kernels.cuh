@@ -62,6 +62,12 @@ struct net_params
 	clock_state * clock;
 	float * dt_ring;
 	int * err;
+	uint4 const * slices;    // tile-major 16-bit slices (window_flat)
+	uint2 const * slice_rec; // [n][ntiles] { first vector, length } (window_flat)
+	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
+	uint2 * wtab;            // [ntiles][ecap] the window's arrivals per tile (stage_window)
+	int * wsteps;            // [MAX_WINDOW + 2] first arrival of every step, validity flag
+	int ecap;                // arrivals per window wtab holds (0: no stage_window)
 };
 
 template <typename T>

@@ -230,7 +230,13 @@ struct spk_net
 	// window kernel of non-plastic models: window_flat (staged arrival table, work-balanced
 	// tiles, neuron state in shared memory) where it applies, else window_counts
 	bool flat = false;
-	int flat_tmax = 0; // the largest tile of the flat tiling
+	int flat_tmax = 0;   // the largest tile of the flat tiling
+	int flat_smem = 0;   // dynamic shared memory of a window_flat launch
+	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
+	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
+	dbuf wtab, wsteps;      // per-window arrival tables of stage_window
+	int ecap = 0;           // arrivals per window stage_window handles (0: off)
+	int stage_chunk = 0;    // arrivals a stage_window CTA transposes at once
 
 	~spk_net()
 	{
@@ -258,6 +264,12 @@ struct spk_net
 		p.clock = clock.as<spk::clock_state>();
 		p.dt_ring = dt_ring.as<float>();
 		p.err = err.as<int>();
+		p.slices = slices.as<uint4 const>();
+		p.slice_rec = slice_rec.as<uint2 const>();
+		p.tile_inputs = tile_inputs.as<int const>();
+		p.wtab = wtab.as<uint2>();
+		p.wsteps = wsteps.as<int>();
+		p.ecap = ecap;
 		return p;
 	}
 
@@ -265,7 +277,7 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes();
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + wtab.bytes + wsteps.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -275,7 +287,7 @@ struct spk_net
 
 	int window_smem() const
 	{
-		if( flat ) return (int)spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax );
+		if( flat ) return flat_smem;
 		int const classes = this->classes();
 		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
 		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
@@ -315,7 +327,15 @@ struct spk_net
 		if constexpr( Model::neuron::input_classes > 0 )
 			if( flat )
 			{
-				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) );
+				// all the shared memory a CTA can have: what the fixed parts leave over
+				// becomes slice buffers
+				int optin = 0;
+				CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
+				cudaFuncAttributes fa{};
+				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model> ) );
+				flat_smem = optin - (int)fa.sharedSizeBytes;
+				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
+				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
 				return;
 			}
 		with_window_kernel<Model>( [&]( auto kernel ) {
@@ -345,7 +365,14 @@ struct spk_net
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
 		}
 		else if( flat )
-			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, flat_tmax );
+		{
+			if( ecap > 0 )
+			{
+				spk::stage_window<<<2 * sms, 256, spk::stage_window_smem( tc.ntiles, stage_chunk ), stream>>>( p, L, stage_chunk );
+				CK( cudaGetLastError() );
+			}
+			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+		}
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
 		CK( cudaGetLastError() );
@@ -602,13 +629,16 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	// equal tiles, SPK_KERNEL=direct selects window_counts)
 	net.flat = false;
 	char const * kern = getenv( "SPK_KERNEL" );
-	if( net.model != SPK_BRUNEL_PLUS && width < spk::FLAT_MAX_WIDTH && !( kern && !strcmp( kern, "direct" ) ) )
+	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) )
 	{
 		int optin = 0;
 		CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net.device ) );
-		long long const room = (long long)optin - 4096 - (long long)spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), 0 );
-		long long const per_neuron8 = 8LL * 4 * ( net.classes() + net.neuron_attrs() ) + 1; // bytes x 8 per neuron
-		int const tmax = (int)std::min<long long>( spk::FLAT_MAX_TILE, room > 0 ? room * 8 / per_neuron8 / 32 * 32 : 0 );
+		// largest tile whose counters, state, table and two minimal slice buffers fit (with
+		// room for the kernel's static shared memory), and whose counter indices fit 16 bits
+		int tmax = spk::FLAT_MAX_TILE;
+		while( tmax >= 128 && ( spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), tmax ) + 4096 > (size_t)optin ||
+		                        (long long)net.classes() * tmax >= spk::SLICE_PAD ) )
+			tmax -= 32;
 		if( tmax >= 128 )
 		{
 			char const * tiling = getenv( "SPK_TILES" );
@@ -648,6 +678,71 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	net.configure();
 }
 
+template <typename Model>
+void fill_slices( spk_net & net, dbuf const & bases )
+{
+	if constexpr( Model::neuron::input_classes > 0 )
+	{
+		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
+		spk::slice_fill<Model><<<blocks, 256, 0, net.stream>>>(
+		    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
+		    bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
+		CK( cudaGetLastError() );
+	}
+}
+
+// the tile-major slices of window_flat, from the ELL rows and their pivots
+void build_slices( spk_net & net )
+{
+	int const nt = net.tc.ntiles;
+	net.slice_rec.alloc( (size_t)net.n * nt * sizeof( uint2 ) );
+	dbuf totals, bases;
+	totals.alloc( (size_t)nt * 8 );
+	bases.alloc( (size_t)nt * 8 );
+	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>() );
+	CK( cudaGetLastError() );
+	spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
+	CK( cudaGetLastError() );
+	std::vector<unsigned long long> tot( nt ), base( nt );
+	CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
+	CK( cudaStreamSynchronize( net.stream ) );
+	unsigned long long all = 0;
+	for( int j = 0; j < nt; j++ )
+	{
+		base[j] = all;
+		all += tot[j];
+	}
+	require( all < ( 1ULL << 32 ), "graph too large for 32-bit slice records" );
+	std::vector<int> inputs( nt );
+	for( int j = 0; j < nt; j++ ) inputs[j] = tot[j] > 0;
+	net.tile_inputs.alloc( (size_t)nt * 4 );
+	CK( cudaMemcpyAsync( net.tile_inputs.p, inputs.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
+	// stage_window: window tables for up to FLAT_STAGE_CAP arrivals (SPK_STAGE=cta: off)
+	char const * stage = getenv( "SPK_STAGE" );
+	net.ecap = 0;
+	if( nt <= 1024 && (long long)net.max_window() * nt + 1 <= spk::FLAT_SCRATCH && !( stage && !strcmp( stage, "cta" ) ) )
+	{
+		net.stage_chunk = (int)std::min<long long>( 32, ( 49152 - 1024 - (long long)spk::FLAT_SCRATCH * 4 ) / ( nt * 8LL + 4 ) );
+		if( net.stage_chunk >= 1 )
+		{
+			net.ecap = spk::FLAT_STAGE_CAP;
+			net.wtab.alloc( (size_t)nt * net.ecap * sizeof( uint2 ) );
+			net.wsteps.alloc( ( spk::MAX_WINDOW + 2 ) * sizeof( int ) );
+			CK( cudaMemsetAsync( net.wsteps.p, 0, net.wsteps.bytes, net.stream ) );
+		}
+	}
+	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ) );
+	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)nt * 8, cudaMemcpyHostToDevice, net.stream ) );
+	switch( net.model )
+	{
+	case SPK_VOGELS_ABBOTT: fill_slices<spice::vogels_abbott>( net, bases ); break;
+	case SPK_BRUNEL: fill_slices<spice::brunel>( net, bases ); break;
+	case SPK_SYNTH: fill_slices<spice::synth>( net, bases ); break;
+	default: break;
+	}
+	CK( cudaStreamSynchronize( net.stream ) ); // totals and bases are freed on return
+}
+
 void enqueue_pivots( spk_net & net )
 {
 	if( net.n == 0 ) return;
@@ -658,6 +753,7 @@ void enqueue_pivots( spk_net & net )
 	else
 		CK( cudaMemsetAsync( net.pivots.p, 0, net.pivots.bytes, net.stream ) );
 	CK( cudaGetLastError() );
+	if( net.flat ) build_slices( net );
 }
 
 void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned long long seed, int * d_edges, dbuf & conns_dev )

@@ -242,21 +242,29 @@ def test_errors():
 
 
 # ----------------------------------------------------------------------- window kernel paths
-@pytest.mark.parametrize("n,delay,steps", [
-    (400_000, 15, 60),     # ~2000 arrivals per step: window tables split into segments
-    (1_700_000, 4, 24),    # > 8192 arrivals in one step: the direct path inside window_flat
+@pytest.mark.parametrize("n,delay,steps,stage", [
+    (60_000, 15, 60, None),      # ~300 arrivals per step: one table per window from stage_window
+    (150_000, 15, 60, None),     # ~750 per step: stage_window's table read in two segments
+    (400_000, 15, 60, None),     # ~2000 per step: more than stage_window holds, per-CTA staging
+    (150_000, 15, 60, "cta"),    # per-CTA staging throughout
+    (1_700_000, 4, 24, None),    # > 8192 arrivals in one step: the direct path inside window_flat
 ])
-def test_flat_kernel_matches_direct_kernel(n, delay, steps):
-    """window_flat (staged table, balanced tiles) against window_counts, itself checked
-    against the oracle above, on nets too large for the oracle to step quickly."""
+def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage):
+    """window_flat (staged table, balanced tiles, slice buffers) against window_counts,
+    itself checked against the oracle above, on nets too large for the oracle to step
+    quickly."""
     layout = Layout(n, 16.0 / n)
-    a = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
+    if stage:
+        os.environ["SPK_STAGE"] = stage
+    try:
+        a = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
+    finally:
+        os.environ.pop("SPK_STAGE", None)
     os.environ["SPK_KERNEL"] = "direct"
     try:
         b = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
     finally:
         del os.environ["SPK_KERNEL"]
-    assert a.info().num_tiles != b.info().num_tiles or a.info().tile_size != b.info().tile_size
     ca, ia = a.run_record(steps, cap=n * steps // 50)
     cb, ib = b.run_record(steps, cap=n * steps // 50)
     assert ca.max() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
