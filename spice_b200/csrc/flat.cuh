@@ -35,6 +35,7 @@
 
 namespace spk
 {
+constexpr int FLAT_THREADS = 1024;  // threads of a window_flat CTA (one CTA per SM)
 constexpr int FLAT_ENT_CAP = 8192;  // staged arrivals per segment of a window
 constexpr int FLAT_SCRATCH = 4096;  // per-(step, source tile) counts staged at once
 constexpr int FLAT_MAX_TILE = 4064; // slice lengths fit the table's 12-bit field
@@ -43,12 +44,16 @@ constexpr int FLAT_P_BITS = 20;     // vector offsets inside a step held in the 
 constexpr int FLAT_STAGE_CAP = 16384; // arrivals per window stage_window stages
 constexpr unsigned short SLICE_PAD = 0xFFFFu;
 
-// shared memory of a CTA: counters [classes][span], neuron state [attrs][span], fired bits,
-// arrival table, staging scratch, then two slice buffers in what is left
+// shared memory of a CTA: neuron state [attrs][span], fired bits [2][words]; tiles with
+// inputs add counters [classes][span], the arrival table, staging scratch and two slice
+// buffers in what is left
+__host__ __device__ inline size_t flat_state_bytes( int attrs, int span )
+{
+	return (size_t)attrs * span * 4 + 2 * ( ( (size_t)span + 31 ) / 32 ) * 4;
+}
 __host__ __device__ inline size_t flat_fixed_bytes( int classes, int attrs, int span )
 {
-	size_t const words = ( (size_t)span + 31 ) / 32;
-	size_t b = (size_t)( classes + attrs ) * span * 4 + words * 4;
+	size_t b = flat_state_bytes( attrs, span ) + (size_t)classes * span * 4;
 	b = ( b + 15 ) & ~(size_t)15;
 	return b + (size_t)FLAT_ENT_CAP * 8 + (size_t)FLAT_SCRATCH * 4;
 }
@@ -60,8 +65,36 @@ inline size_t flat_smem_bytes( int classes, int attrs, int tmax )
 // ------------------------------------------------------------------------------------
 // building the slices (once per net)
 // ------------------------------------------------------------------------------------
-// vectors of every (src, tile) slice, from the ELL pivots, into rec[].x
-__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2 * rec )
+// 16-byte vectors of a slice of `len` targets: a list of 16-bit indices (dense == 0) or
+// a bitmap of the tile's `words` receiving 32-neuron words (dense == 1, none if len == 0)
+__host__ __device__ inline unsigned slice_vecs( unsigned len, int words, int dense )
+{
+	if( !dense ) return ( len + 7 ) >> 3;
+	return len ? (unsigned)( ( words + 3 ) / 4 ) : 0u;
+}
+
+// lowest and highest tile-local target of every tile over all rows (tiles without
+// inputs keep lo = INT_MAX)
+__global__ void tile_target_range(
+    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first, int * lo, int * hi )
+{
+	long long const total = (long long)n * ntiles;
+	for( long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x )
+	{
+		long long const src = e / ntiles;
+		int const j = (int)( e % ntiles );
+		unsigned const * pv = pivots + src * ( ntiles + 1 ) + j;
+		if( pv[1] > pv[0] )
+		{
+			int const * row = edges + src * width;
+			atomicMin( lo + j, row[pv[0]] - tile_first[j] );
+			atomicMax( hi + j, row[pv[1] - 1] - tile_first[j] );
+		}
+	}
+}
+
+// vectors of every (src, tile) slice, from the ELL pivots, into rec[].x; rec[].y = length
+__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, int2 const * bm_range, int dense, uint2 * rec )
 {
 	long long const total = (long long)n * ntiles;
 	for( long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x )
@@ -69,7 +102,7 @@ __global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2
 		long long const src = e / ntiles, j = e % ntiles;
 		unsigned const * pv = pivots + src * ( ntiles + 1 ) + j;
 		unsigned const len = pv[1] - pv[0];
-		rec[e] = make_uint2( ( len + 7 ) >> 3, len );
+		rec[e] = make_uint2( slice_vecs( len, bm_range[j].y, dense ), len );
 	}
 }
 
@@ -117,10 +150,11 @@ __global__ void __launch_bounds__( 1024 ) slice_offsets( int n, int ntiles, uint
 	}
 }
 
-// one warp per source row: rebase rec[] to global vector indices and write every slice
-template <typename Model>
+// one warp per source row: rebase rec[] to global vector indices and write every slice.
+// Lists: rec.y = length. Bitmaps: rec.y = 1 | class << 1 for a slice with targets, 0 else.
+template <typename Model, bool Dense>
 __global__ void __launch_bounds__( 256 ) slice_fill(
-    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first,
+    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first, int2 const * bm_range,
     unsigned long long const * tile_base, uint2 * rec, unsigned short * slices )
 {
 	using N = typename Model::neuron;
@@ -135,15 +169,32 @@ __global__ void __launch_bounds__( 256 ) slice_fill(
 	{
 		uint2 const r = rec[(long long)src * ntiles + j];
 		unsigned long long const first = tile_base[j] + r.x;
+		unsigned const y = Dense ? ( r.y ? 1u | (unsigned)cls << 1 : 0u ) : r.y;
 		__syncwarp();
-		if( lane == 0 ) rec[(long long)src * ntiles + j] = make_uint2( (unsigned)first, r.y );
+		if( lane == 0 ) rec[(long long)src * ntiles + j] = make_uint2( (unsigned)first, y );
 		if( r.y == 0 ) continue;
 		int const d0 = tile_first[j], span = tile_first[j + 1] - d0;
 		unsigned const lo = pv[j];
-		unsigned short * out = slices + first * 8;
-		int const padded = (int)( ( r.y + 7 ) & ~7u );
-		for( int e = lane; e < padded; e += 32 )
-			out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
+		if constexpr( Dense )
+		{
+			unsigned * out = reinterpret_cast<unsigned *>( slices ) + first * 4;
+			int2 const br = bm_range[j];
+			int const padded = (int)slice_vecs( r.y, br.y, 1 ) * 4;
+			for( int e = lane; e < padded; e += 32 ) out[e] = 0u;
+			__syncwarp();
+			for( int e = lane; e < (int)r.y; e += 32 )
+			{
+				int const local = row[lo + e] - d0 - 32 * br.x;
+				atomicOr( out + ( local >> 5 ), 1u << ( local & 31 ) );
+			}
+		}
+		else
+		{
+			unsigned short * out = slices + first * 8;
+			int const padded = (int)( ( r.y + 7 ) & ~7u );
+			for( int e = lane; e < padded; e += 32 )
+				out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
+		}
 	}
 }
 
@@ -276,15 +327,18 @@ __global__ void __launch_bounds__( 256 ) stage_window( net_params p, int L, int 
 // ------------------------------------------------------------------------------------
 // window kernel
 // ------------------------------------------------------------------------------------
-// table[g] = { first vector of the slice, length | vector offset inside its step << 12 }
-__device__ __forceinline__ int ent_len( int2 e ) { return e.y & 0xFFF; }
-__device__ __forceinline__ int ent_vec( int2 e ) { return ( ent_len( e ) + 7 ) >> 3; }
+// table[g] = { first vector of the slice, low | vector offset inside its step << 12 } with
+// low = length (lists) or 1 | class << 1 for a bitmap with targets (bitmaps: `wv` vectors
+// each; wv == 0 selects lists)
+__device__ __forceinline__ int ent_low( int2 e ) { return e.y & 0xFFF; }
+__device__ __forceinline__ int ent_vec( int2 e, int wv ) { return wv ? ( ent_low( e ) & 1 ) * wv : ( ent_low( e ) + 7 ) >> 3; }
+__device__ __forceinline__ int ent_cls( int2 e ) { return ( ent_low( e ) >> 1 ) & 7; }
 __device__ __forceinline__ int ent_off( int2 e ) { return (int)( (unsigned)e.y >> 12 ); }
 
 __device__ __forceinline__ int stage_arrivals(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int & nent_out, int * scratch );
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch );
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int wv );
 
 // Stage the arrivals of the steps [ks, L) of the window starting at t0, as many whole
 // steps as fit FLAT_ENT_CAP and keep their vector offsets within FLAT_P_BITS. Returns
@@ -293,7 +347,7 @@ __device__ __forceinline__ int stage_offsets(
 // k counted from the segment start, for k in [ks, ke].
 __device__ __forceinline__ int stage_table(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int * step_vec,
-    int * scratch )
+    int * scratch, int wv )
 {
 	constexpr int B = 8; // loads in flight per thread
 	int const tid = threadIdx.x, nt = blockDim.x;
@@ -323,7 +377,7 @@ __device__ __forceinline__ int stage_table(
 	}
 	else
 		ke = stage_arrivals( p, cnts, table, tile, t0, ks, L, step_begin, nent, scratch );
-	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch );
+	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, wv );
 }
 
 // Per-CTA staging (when stage_window did not run or the window did not fit): the
@@ -410,13 +464,13 @@ __device__ __forceinline__ int stage_arrivals(
 // A step whose vectors do not fit the offset field ends the segment before it; returns
 // the segment's end.
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch )
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int wv )
 {
 	int const tid = threadIdx.x, nt = blockDim.x;
 	int const per = ( nent + nt - 1 ) / nt;
 	int const g0 = min( nent, tid * per ), g1 = min( nent, g0 + per );
 	int run = 0;
-	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g] );
+	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g], wv );
 	int vtotal;
 	int const my_first = block_exclusive_scan( run, scratch, &vtotal );
 	run_first[tid] = my_first;
@@ -429,7 +483,7 @@ __device__ __forceinline__ int stage_offsets(
 		{
 			int const owner = g / per;
 			v = run_first[owner];
-			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h] );
+			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h], wv );
 		}
 		step_vec[k] = v;
 	}
@@ -443,8 +497,8 @@ __device__ __forceinline__ int stage_offsets(
 			while( step_begin[k + 1] <= g ) k++;
 			int2 e = table[g];
 			unsigned const rel = (unsigned)( v - step_vec[k] );
-			int const nv = ent_vec( e );
-			e.y = ent_len( e ) | (int)( ( rel & ( ( 1u << FLAT_P_BITS ) - 1 ) ) << 12 );
+			int const nv = ent_vec( e, wv );
+			e.y = ent_low( e ) | (int)( ( rel & ( ( 1u << FLAT_P_BITS ) - 1 ) ) << 12 );
 			table[g] = e;
 			v += nv;
 		}
@@ -458,7 +512,7 @@ __device__ __forceinline__ int stage_offsets(
 
 // one past the last entry of the piece starting at entry `a` of a step whose entries end
 // at `e`: the entries whose vectors fit one buffer of `bufv` vectors together
-__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv )
+__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv, int wv )
 {
 	int const pa = ent_off( table[a] );
 	int lo = a, hi = e; // f(g) = off(g) + vec(g) - pa <= bufv holds for g = a
@@ -466,7 +520,7 @@ __device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int 
 	{
 		int const mid = ( lo + hi ) >> 1;
 		int2 const m = table[mid];
-		if( ent_off( m ) + ent_vec( m ) - pa <= bufv )
+		if( ent_off( m ) + ent_vec( m, wv ) - pa <= bufv )
 			lo = mid;
 		else
 			hi = mid;
@@ -484,7 +538,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wa
 
 // copy the slices of entries [a, b) into buf: groups of 8 lanes per entry, lane q copies
 // vectors q, q + 8, ... (a warp instruction touches 4 slices, not 32)
-__device__ __forceinline__ void issue_piece( net_params const & p, int2 const * table, int a, int b, uint4 * buf )
+__device__ __forceinline__ void issue_piece( net_params const & p, int2 const * table, int a, int b, uint4 * buf, int wv )
 {
 	if( a >= b ) return;
 	int const pa = ent_off( table[a] );
@@ -492,7 +546,7 @@ __device__ __forceinline__ void issue_piece( net_params const & p, int2 const * 
 	for( int g = a + (int)( threadIdx.x >> 3 ); g < b; g += groups )
 	{
 		int2 const e = table[g];
-		int const nv = ent_vec( e );
+		int const nv = ent_vec( e, wv );
 		uint4 const * src = p.slices + (unsigned)e.x;
 		uint4 * dst = buf + ( ent_off( e ) - pa );
 		for( int j = q; j < nv; j += 8 ) cp_async16( dst + j, src + j );
@@ -527,6 +581,74 @@ __device__ __forceinline__ int piece_vectors( int2 const * table, int a, int b, 
 {
 	if( a >= b ) return 0;
 	return ( b < e ? ent_off( table[b] ) : step_vectors ) - ent_off( table[a] );
+}
+
+// 32 x 32 bit transpose across a warp: afterwards bit j of lane l is bit l of lane j
+__device__ __forceinline__ unsigned warp_transpose32( unsigned x, int lane )
+{
+#pragma unroll
+	for( int s = 16; s >= 1; s >>= 1 )
+	{
+		unsigned const m = s == 16 ? 0x0000FFFFu : s == 8 ? 0x00FF00FFu : s == 4 ? 0x0F0F0F0Fu : s == 2 ? 0x33333333u : 0x55555555u;
+		unsigned const y = __shfl_xor_sync( 0xffffffffu, x, s );
+		// lanes with bit s set keep their high halves and take the partner's high halves
+		// shifted down, the others keep their low halves and take the partner's low halves
+		// shifted up (~m >> s == m for these masks)
+		bool const up = lane & s;
+		unsigned const keep = up ? ~m : m;
+		unsigned const z = up ? y >> s : y << s;
+		x = ( x & keep ) | ( z & ~keep );
+	}
+	return x;
+}
+
+// Bitmap counting. Slots [s0, s1) lie in `buf` from slot `base` on, `ww` words each. For
+// bitmap word w, lane l adds the words of slots s0 + l, s0 + l + 32, ... into four bit
+// planes (a per-bit counter up to 15), in rounds of 15 slots per lane; transposing a plane
+// makes lane l's popcount the number of planes' bits l over all lanes. Returns this lane's
+// count for bit `lane` of word w.
+__device__ __forceinline__ unsigned bitmap_count( unsigned const * buf, int base, int s0, int s1, int ww, int w, int lane )
+{
+	unsigned total = 0;
+	for( int r0 = s0; r0 < s1; r0 += 15 * 32 )
+	{
+		int const r1 = min( s1, r0 + 15 * 32 );
+		unsigned p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+		for( int s = r0 + lane; s < r1; s += 32 )
+		{
+			unsigned c = buf[( s - base ) * ww + w];
+			unsigned t = p0 & c;
+			p0 ^= c;
+			c = t;
+			t = p1 & c;
+			p1 ^= c;
+			c = t;
+			t = p2 & c;
+			p2 ^= c;
+			p3 ^= t; // no carry out: a lane adds at most 15 words
+		}
+		// planes needed for the largest lane count (uniform across the warp)
+		int const most = ( r1 - r0 + 31 ) >> 5;
+		if( most >= 8 )
+		{
+			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane ), c = warp_transpose32( p2, lane ),
+			               d = warp_transpose32( p3, lane );
+			total += __popc( a ) + ( __popc( b ) << 1 ) + ( __popc( c ) << 2 ) + ( __popc( d ) << 3 );
+		}
+		else if( most >= 4 )
+		{
+			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane ), c = warp_transpose32( p2, lane );
+			total += __popc( a ) + ( __popc( b ) << 1 ) + ( __popc( c ) << 2 );
+		}
+		else if( most >= 2 )
+		{
+			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane );
+			total += __popc( a ) + ( __popc( b ) << 1 );
+		}
+		else
+			total += __popc( warp_transpose32( p0, lane ) );
+	}
+	return total;
 }
 
 // neuron state of the tile: shared memory [attrs][span] <-> registers / global memory
@@ -589,13 +711,14 @@ struct smem_state
 	}
 };
 
-template <typename Model>
-__global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
+template <typename Model, bool Dense>
+__global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
 {
 	using N = typename Model::neuron;
 	using Tup = typename N::template apply<reg_tuple>;
 	constexpr int C = N::input_classes;
 	static_assert( C >= 1, "window_flat needs a model with input classes" );
+	static_assert( !Dense || C <= 4, "bitmap slices carry up to four input classes" );
 
 	extern __shared__ __align__( 128 ) unsigned char smem[];
 	__shared__ int scratch[33];
@@ -604,16 +727,21 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 	__shared__ float s_c, s_sum;
 	__shared__ int step_begin[MAX_WINDOW + 1];
 	__shared__ int step_vec[MAX_WINDOW + 1];
+	__shared__ int s_cslots[MAX_WINDOW][4]; // bitmaps: slots of every input class per step
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
 	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
+	// bitmaps: words [bw0, bw0 + bwn) of the tile hold all its targets, wv vectors each
+	int2 const brange = Dense ? __ldg( p.bm_range + tile ) : make_int2( 0, 0 );
+	int const bw0 = brange.x, bwn = brange.y;
+	int const wv = Dense ? max( 1, ( bwn + 3 ) >> 2 ) : 0;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
 	snn_info const info{ p.n };
 
-	unsigned * cnt = reinterpret_cast<unsigned *>( smem );                                // [C][span]
-	unsigned char * state = reinterpret_cast<unsigned char *>( cnt + C * span );           // [attrs][span]
-	unsigned * bits = reinterpret_cast<unsigned *>( state + (size_t)N::size * span * 4 ); // [words]
+	unsigned char * state = smem;                                                          // [attrs][span]
+	unsigned * bits2 = reinterpret_cast<unsigned *>( state + (size_t)N::size * span * 4 ); // [2][words]
+	unsigned * cnt = bits2 + 2 * words;                                                    // [C][span], inputs only
 	size_t const fixed = flat_fixed_bytes( C, (int)N::size, span );
 	int2 * table = reinterpret_cast<int2 *>( smem + fixed - (size_t)FLAT_ENT_CAP * 8 - (size_t)FLAT_SCRATCH * 4 );
 	unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
@@ -625,22 +753,49 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 	long long const t0 = s_t0;
 	smem_state<N>::from_global( p.attr, d0, span, state );
 	// counters start at zero; the update phase zeroes every counter it consumes
-	for( int x = tid; x < C * span; x += nt ) cnt[x] = 0;
+	if( inputs )
+		for( int x = tid; x < C * span; x += nt ) cnt[x] = 0;
 	__syncthreads();
 
 	int ks = 0;
 	while( ks < L )
 	{
-		int const ke = inputs ? stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch ) : L;
+		int const ke = inputs ? stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch, wv ) : L;
 		bool const direct = ke == ks; // step ks alone exceeds the table
 		int const kend = direct ? ks + 1 : ke;
 		bool const piped = inputs && !direct; // slices flow through the two buffers
+		if( Dense && piped )
+		{
+			// bitmaps of every input class per step (slots ascend with the source id, and so
+			// does the class)
+			for( int x = tid; x < ( kend - ks ) * 4; x += nt ) s_cslots[x >> 2][x & 3] = 0;
+			__syncthreads();
+			int const nent = step_begin[kend - ks];
+			for( int g = tid; g < nent; g += nt )
+			{
+				int2 const e = table[g];
+				if( ent_low( e ) & 1 )
+				{
+					int lo = 0, hi = kend - ks; // step of g: last k with step_begin[k] <= g
+					while( hi - lo > 1 )
+					{
+						int const mid = ( lo + hi ) >> 1;
+						if( step_begin[mid] <= g )
+							lo = mid;
+						else
+							hi = mid;
+					}
+					atomicAdd( &s_cslots[lo][ent_cls( e )], 1 );
+				}
+			}
+			__syncthreads();
+		}
 
 		// first piece [a, b) of step k
 		auto first_piece = [&]( int k, int & a, int & b ) {
 			a = step_begin[k - ks];
 			int const e = step_begin[k + 1 - ks];
-			b = a < e ? piece_end( table, a, e, bufv ) : a;
+			b = a < e ? piece_end( table, a, e, bufv, wv ) : a;
 		};
 		if( piped )
 		{
@@ -649,7 +804,7 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 			{
 				int a, b;
 				first_piece( k, a, b );
-				issue_piece( p, table, a, b, ( k & 1 ) ? buf1 : buf0 );
+				issue_piece( p, table, a, b, ( k & 1 ) ? buf1 : buf0, wv );
 			}
 			cp_async_commit();
 			cp_async_wait_all();
@@ -676,23 +831,64 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 				{
 					int const e = step_begin[k + 1 - ks];
 					int const sv = step_vec[k + 1 - ks] - step_vec[k - ks];
+					// bitmaps: the warp that owns word w counts it for all classes; the
+					// counts land in the counter rows the update reads
+					auto count_piece = [&]( int a, int b ) {
+						if constexpr( Dense )
+						{
+							if( a >= b ) return;
+							int const slot0 = ent_off( table[a] ) / wv;
+							int const slot1 = ( b < e ? ent_off( table[b] ) : sv ) / wv;
+							unsigned const * bw = reinterpret_cast<unsigned const *>( bk );
+							// class 0 = all slots minus the other classes (fewer planes to move).
+							// Warp `warp` counts the tile words it updates below (warp + r nw),
+							// so no barrier is needed between counting and the update.
+							for( int tw = warp; tw < bw0 + bwn; tw += nw )
+							{
+								if( tw < bw0 ) continue;
+								int const w = tw - bw0;
+								int const local = ( tw << 5 ) + lane;
+								unsigned rest = 0;
+								int c0 = s_cslots[k - ks][0];
+#pragma unroll
+								for( int c = 1; c < C; c++ )
+								{
+									int const c1 = c0 + s_cslots[k - ks][c];
+									int const lo = max( c0, slot0 ), hi = min( c1, slot1 );
+									if( lo < hi )
+									{
+										unsigned const m = bitmap_count( bw, slot0, lo, hi, wv * 4, w, lane );
+										if( local < span ) cnt[c * span + local] += m;
+										rest += m;
+									}
+									c0 = c1;
+								}
+								unsigned const all = bitmap_count( bw, slot0, slot0, slot1, wv * 4, w, lane );
+								if( local < span ) cnt[local] += all - rest;
+							}
+						}
+						else
+							count_buffer( bk, piece_vectors( table, a, b, e, sv ), cnt );
+					};
 					int a, b;
 					first_piece( k, a, b );
-					count_buffer( bk, piece_vectors( table, a, b, e, sv ), cnt );
+					count_piece( a, b );
 					while( b < e ) // the rest of a step larger than a buffer
 					{
 						__syncthreads(); // bk is free
 						a = b;
-						b = piece_end( table, a, e, bufv );
-						issue_piece( p, table, a, b, bk );
+						b = piece_end( table, a, e, bufv, wv );
+						issue_piece( p, table, a, b, bk, wv );
 						cp_async_commit();
 						cp_async_wait_all();
 						__syncthreads();
-						count_buffer( bk, piece_vectors( table, a, b, e, sv ), cnt );
+						count_piece( a, b );
 					}
 				}
 			}
-			__syncthreads(); // counts complete; the previous step's compaction is done
+			// counts complete (bitmaps: every warp counted its own words, no barrier needed)
+			if( !Dense || !piped ) __syncthreads();
+			unsigned * bits = bits2 + ( k & 1 ) * words; // the compaction of step k - 1 reads the other half
 
 			// update: warp w owns neurons [32 w, 32 w + 32) + 32 nw * round; one bit word each
 			for( int base = warp * 32; base < span; base += nw * 32 )
@@ -705,7 +901,7 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 					smem_state<N>::load( st, state, span, local );
 					uint32_t const i = (uint32_t)( d0 + local );
 					reg_iter<Tup> it{ st, i };
-					if( arrivals )
+					if( inputs && arrivals )
 #pragma unroll
 						for( int c = 0; c < C; c++ )
 						{
@@ -731,7 +927,7 @@ __global__ void __launch_bounds__( 512, 1 ) window_flat( net_params p, int L, fl
 				// step k + 2 into the buffer step k was counted from (done: barrier above)
 				int a, b;
 				first_piece( k + 2, a, b );
-				issue_piece( p, table, a, b, bk );
+				issue_piece( p, table, a, b, bk, wv );
 				cp_async_commit();
 			}
 			// ascending compaction by the last warp, without a further barrier: 32 words per

@@ -232,8 +232,10 @@ struct spk_net
 	bool flat = false;
 	int flat_tmax = 0;   // the largest tile of the flat tiling
 	int flat_smem = 0;   // dynamic shared memory of a window_flat launch
+	bool dense = false;  // slices are tile bitmaps (else 16-bit index lists)
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
+	dbuf bm_range;          // [ntiles] receiving word range of every tile (bitmaps)
 	dbuf wtab, wsteps;      // per-window arrival tables of stage_window
 	int ecap = 0;           // arrivals per window stage_window handles (0: off)
 	int stage_chunk = 0;    // arrivals a stage_window CTA transposes at once
@@ -267,6 +269,7 @@ struct spk_net
 		p.slices = slices.as<uint4 const>();
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
+		p.bm_range = bm_range.as<int2 const>();
 		p.wtab = wtab.as<uint2>();
 		p.wsteps = wsteps.as<int>();
 		p.ecap = ecap;
@@ -277,7 +280,8 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + wtab.bytes + wsteps.bytes;
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + bm_range.bytes + wtab.bytes +
+		           wsteps.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -331,11 +335,18 @@ struct spk_net
 				// becomes slice buffers
 				int optin = 0;
 				CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
-				cudaFuncAttributes fa{};
-				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model> ) );
+				cudaFuncAttributes fa{}, fb{};
+				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model, false> ) );
 				flat_smem = optin - (int)fa.sharedSizeBytes;
+				if constexpr( Model::neuron::input_classes <= 4 )
+				{
+					CK( cudaFuncGetAttributes( &fb, spk::window_flat<Model, true> ) );
+					flat_smem = std::min( flat_smem, optin - (int)fb.sharedSizeBytes );
+				}
 				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
-				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				CK( cudaFuncSetAttribute( spk::window_flat<Model, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				if constexpr( Model::neuron::input_classes <= 4 )
+					CK( cudaFuncSetAttribute( spk::window_flat<Model, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
 				return;
 			}
 		with_window_kernel<Model>( [&]( auto kernel ) {
@@ -371,7 +382,14 @@ struct spk_net
 				spk::stage_window<<<2 * sms, 256, spk::stage_window_smem( tc.ntiles, stage_chunk ), stream>>>( p, L, stage_chunk );
 				CK( cudaGetLastError() );
 			}
-			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+			if constexpr( Model::neuron::input_classes <= 4 )
+				if( dense )
+				{
+					spk::window_flat<Model, true><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+					CK( cudaGetLastError() );
+					return;
+				}
+			spk::window_flat<Model, false><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
 		}
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
@@ -505,8 +523,10 @@ struct cost_segment
 	double cost;
 };
 
-// one neuron update against one delivered synapse, for tile balancing
-constexpr double UPDATE_COST = 32.0;
+// one neuron update against one synapse of in-degree, for tile balancing. Measured on
+// B200 (Brunel, 1e9 synapses): a Poisson source (one counter-RNG draw per step) costs
+// about as much per window as 1000 synapses of in-degree of a receiving neuron.
+constexpr double UPDATE_COST = 1000.0;
 
 // expected in-degree of every neuron of a layout (constant over stretches of populations)
 std::vector<cost_segment> layout_costs( spice::util::layout const & l )
@@ -542,11 +562,14 @@ std::vector<cost_segment> adjacency_costs( int const * edges, long long n, long 
 	return segs;
 }
 
-// Cut [0, n) into contiguous tiles of about equal work, at most tmax neurons each,
-// aiming at no more tiles than SMs (every tile scans every arrival of a step).
-std::vector<int> balanced_tiles( std::vector<cost_segment> const & segs, long long n, int sms, int tmax )
+// Cut [0, n) into contiguous tiles of about equal work, aiming at no more tiles than SMs
+// (every tile with inputs scans every arrival of a step). Tiles never mix neurons with
+// and without incoming synapses (cost == UPDATE_COST): tiles with inputs hold at most
+// tmax_in neurons, tiles without at most tmax_free (they keep only neuron state).
+std::vector<int> balanced_tiles( std::vector<cost_segment> const & segs, long long n, int sms, int tmax_in, int tmax_free )
 {
 	auto seg_end = [&]( size_t i ) { return i + 1 < segs.size() ? segs[i + 1].start : n; };
+	auto is_free = [&]( size_t i ) { return segs[i].cost <= UPDATE_COST; };
 	double total = 0;
 	for( size_t i = 0; i < segs.size(); i++ ) total += ( seg_end( i ) - segs[i].start ) * segs[i].cost;
 	auto cut = [&]( double target ) {
@@ -558,6 +581,13 @@ std::vector<int> balanced_tiles( std::vector<cost_segment> const & segs, long lo
 			double const c = std::max( segs[i].cost, 1e-9 );
 			long long pos = segs[i].start;
 			long long const e = seg_end( i );
+			int const tmax = is_free( i ) ? tmax_free : tmax_in;
+			if( i > 0 && is_free( i ) != is_free( i - 1 ) && pos > start ) // no mixed tiles
+			{
+				first.push_back( (int)pos );
+				start = pos;
+				acc = 0;
+			}
 			while( pos < e )
 			{
 				long long const room = tmax - ( pos - start );
@@ -639,18 +669,27 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 		while( tmax >= 128 && ( spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), tmax ) + 4096 > (size_t)optin ||
 		                        (long long)net.classes() * tmax >= spk::SLICE_PAD ) )
 			tmax -= 32;
+		// tiles without inputs keep only their neuron state and fired bits
+		int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * net.neuron_attrs() + 8 ) ) / 32 * 32 );
 		if( tmax >= 128 )
 		{
 			char const * tiling = getenv( "SPK_TILES" );
 			std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
-			                                                                       : balanced_tiles( segs, n, dev_sms, tmax );
+			                                                                       : balanced_tiles( segs, n, dev_sms, tmax, tmax_free );
 			if( (int)first.size() - 1 < spk::FLAT_SCRATCH )
 			{
+				// the largest tile with inputs sets the shared-memory floor (tiles without
+				// inputs need less than it per neuron)
 				int span = 0;
-				for( size_t i = 0; i + 1 < first.size(); i++ ) span = std::max( span, first[i + 1] - first[i] );
+				size_t si = 0;
+				for( size_t i = 0; i + 1 < first.size(); i++ )
+				{
+					while( si + 1 < segs.size() && segs[si + 1].start <= first[i] ) si++;
+					if( segs[si].cost > UPDATE_COST || first[i + 1] - first[i] <= tmax ) span = std::max( span, first[i + 1] - first[i] );
+				}
 				net.flat = true;
 				net.flat_tmax = ( span + 31 ) / 32 * 32;
-				net.tc = { 512, 1, net.flat_tmax, (int)first.size() - 1 };
+				net.tc = { spk::FLAT_THREADS, 1, net.flat_tmax, (int)first.size() - 1 };
 				set_tiles( net, first );
 			}
 		}
@@ -684,9 +723,15 @@ void fill_slices( spk_net & net, dbuf const & bases )
 	if constexpr( Model::neuron::input_classes > 0 )
 	{
 		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
-		spk::slice_fill<Model><<<blocks, 256, 0, net.stream>>>(
-		    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
-		    bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
+		auto fill = [&]( auto kernel ) {
+			kernel<<<blocks, 256, 0, net.stream>>>(
+			    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
+			    net.bm_range.as<int2>(), bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
+		};
+		if( net.dense )
+			fill( spk::slice_fill<Model, true> );
+		else
+			fill( spk::slice_fill<Model, false> );
 		CK( cudaGetLastError() );
 	}
 }
@@ -699,13 +744,55 @@ void build_slices( spk_net & net )
 	dbuf totals, bases;
 	totals.alloc( (size_t)nt * 8 );
 	bases.alloc( (size_t)nt * 8 );
-	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>() );
-	CK( cudaGetLastError() );
-	spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
-	CK( cudaGetLastError() );
 	std::vector<unsigned long long> tot( nt ), base( nt );
-	CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
-	CK( cudaStreamSynchronize( net.stream ) );
+	// receiving word range of every tile: bitmaps cover only these words
+	{
+		dbuf lo, hi;
+		lo.alloc( (size_t)nt * 4 );
+		hi.alloc( (size_t)nt * 4 );
+		std::vector<int> l( nt, INT_MAX ), h( nt, -1 );
+		CK( cudaMemcpyAsync( lo.p, l.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
+		CK( cudaMemcpyAsync( hi.p, h.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
+		if( net.width > 0 )
+		{
+			spk::tile_target_range<<<4 * net.sms, 256, 0, net.stream>>>(
+			    (int)net.n, (int)net.width, nt, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(), lo.as<int>(), hi.as<int>() );
+			CK( cudaGetLastError() );
+		}
+		CK( cudaMemcpyAsync( l.data(), lo.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
+		CK( cudaMemcpyAsync( h.data(), hi.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
+		CK( cudaStreamSynchronize( net.stream ) );
+		std::vector<int2> r( nt );
+		for( int j = 0; j < nt; j++ ) r[j] = h[j] < 0 ? make_int2( 0, 0 ) : make_int2( l[j] / 32, h[j] / 32 - l[j] / 32 + 1 );
+		net.bm_range.alloc( (size_t)nt * sizeof( int2 ) );
+		CK( cudaMemcpyAsync( net.bm_range.p, r.data(), (size_t)nt * sizeof( int2 ), cudaMemcpyHostToDevice, net.stream ) );
+		CK( cudaStreamSynchronize( net.stream ) );
+	}
+	// vectors per (src, tile) and their per-tile prefix, as lists or as bitmaps
+	auto layout_pass = [&]( int dense ) {
+		spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>(
+		    (int)net.n, nt, net.pivots.as<unsigned>(), net.bm_range.as<int2>(), dense, net.slice_rec.as<uint2>() );
+		CK( cudaGetLastError() );
+		spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
+		CK( cudaGetLastError() );
+		CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
+		CK( cudaStreamSynchronize( net.stream ) );
+		unsigned long long all = 0;
+		for( auto v : tot ) all += v;
+		return all;
+	};
+	// bitmaps where they take fewer bytes than index lists (dense connectivity, p > ~1/16),
+	// SPK_SLICES=list|bitmap forces one
+	char const * mode = getenv( "SPK_SLICES" );
+	bool const can_dense = net.classes() <= 4;
+	unsigned long long const list_vecs = layout_pass( 0 );
+	net.dense = false;
+	if( can_dense && !( mode && !strcmp( mode, "list" ) ) )
+	{
+		unsigned long long const dense_vecs = layout_pass( 1 );
+		net.dense = dense_vecs <= list_vecs || ( mode && !strcmp( mode, "bitmap" ) );
+		if( !net.dense ) layout_pass( 0 );
+	}
 	unsigned long long all = 0;
 	for( int j = 0; j < nt; j++ )
 	{
