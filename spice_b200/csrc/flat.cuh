@@ -10,43 +10,49 @@
 // CTA reads only its own tile's region, two bytes per synapse, already in the form its
 // counters are indexed by.
 //
-//   1. Staging. All arrivals of the window fired before it started, so the CTA stages the
-//      window's arrival table (first vector, length, vector offset inside the step) in
-//      shared memory: per-(step, source tile) spike counts, spike ids, slice records.
-//   2. Prefetch. The slices of step k + 2 are copied into one of two shared-memory
-//      buffers with cp.async while step k is updated, so the loads of a step overlap the
-//      work of the step before it.
-//   3. Counting. Threads walk the step's buffer one 16-byte vector at a time and count
-//      every index with a shared-memory atomic. A step larger than a buffer is counted in
-//      pieces that are loaded synchronously.
-//   4. Update. The tile's neuron state lives in shared memory for the whole window; the
-//      counts are replayed through the model's receive(), the model updates every neuron
-//      and the counters it consumed are zeroed; fired neurons are compacted in ascending
-//      order into the spike ring. Two barriers per step.
+//   1. Staging. All arrivals of the window fired before it started: stage_window (or the
+//      CTA itself) builds the window's arrival table (first vector, length, vector offset
+//      inside the step) in shared memory.
+//   2. Producers. FLAT_PRODUCERS warps copy the slices of step k + 2 into one of three
+//      shared-memory buffers with cp.async while the other warps work on step k, so the
+//      burst of scattered loads that every tile issues at the same time overlaps counting
+//      and updating instead of stalling them.
+//   3. Consumers count step k from its buffer, one 16-byte vector per thread at a time,
+//      with a shared-memory atomic per index; a consumer-only barrier; then they replay
+//      the counts through the model's receive(), update every neuron and zero the
+//      counters they consumed. The tile's neuron state stays in shared memory for the
+//      whole window.
+//   4. A producer warp compacts the fired neurons of step k - 1 in ascending order into
+//      the spike ring. One block-wide barrier per step.
+// A step whose slices exceed a buffer, or whose arrivals exceed the table, runs alone with
+// every warp (pieces loaded synchronously, or the direct path of window_counts).
 // Keeping the state in shared memory lets tile sizes follow the work (balanced tiles): a
 // population without inputs costs little per neuron and gets few, large tiles.
 //
-// Measured on B200 (Brunel, 1e9 synapses): with 4-byte row loads issued one step at a
-// time the counting phase waited on memory for most of a step; the layout and the
-// two-step-ahead copies remove both the wait and half the bytes.
+// Measured on B200 (Brunel, 1e9 synapses): scattered 16-byte copies issue at about one per
+// cycle per SM, and since all tiles issue theirs at the same moment the burst runs near
+// HBM bandwidth; issued by the warps that then count, it sat on every step's critical path.
 #pragma once
 
 #include "kernels.cuh"
 
 namespace spk
 {
-constexpr int FLAT_THREADS = 1024;  // threads of a window_flat CTA (one CTA per SM)
-constexpr int FLAT_ENT_CAP = 8192;  // staged arrivals per segment of a window
-constexpr int FLAT_SCRATCH = 4096;  // per-(step, source tile) counts staged at once
-constexpr int FLAT_MAX_TILE = 4064; // slice lengths fit the table's 12-bit field
-constexpr int FLAT_MIN_BUF = 512;   // vectors per buffer at least (one slice of a full tile)
-constexpr int FLAT_P_BITS = 20;     // vector offsets inside a step held in the table
+constexpr int FLAT_THREADS = 1024;    // threads of a window_flat CTA (one CTA per SM)
+constexpr int FLAT_PRODUCERS = 8;     // warps that copy slices and compact spikes
+constexpr int FLAT_BUFS = 3;          // slice buffers: step k counted, k + 1 ready, k + 2 loading
+constexpr int FLAT_ENT_CAP = 6144;    // staged arrivals per segment of a window
+constexpr int FLAT_SCRATCH = 2560;    // per-(step, source tile) counts staged at once (>= threads)
+constexpr int FLAT_MAX_TILE = 4064;   // slice lengths fit the table's 12-bit field
+constexpr int FLAT_MIN_BUF = 512;     // vectors per buffer at least (one slice of a full tile)
+constexpr int FLAT_P_BITS = 20;       // vector offsets inside a step held in the table
 constexpr int FLAT_STAGE_CAP = 16384; // arrivals per window stage_window stages
 constexpr unsigned short SLICE_PAD = 0xFFFFu;
+static_assert( FLAT_SCRATCH >= FLAT_THREADS, "staging keeps one prefix per thread in the scratch" );
 
 // shared memory of a CTA: neuron state [attrs][span], fired bits [2][words]; tiles with
-// inputs add counters [classes][span], the arrival table, staging scratch and two slice
-// buffers in what is left
+// inputs add counters [classes][span], the arrival table, staging scratch and FLAT_BUFS
+// slice buffers in what is left
 __host__ __device__ inline size_t flat_state_bytes( int attrs, int span )
 {
 	return (size_t)attrs * span * 4 + 2 * ( ( (size_t)span + 31 ) / 32 ) * 4;
@@ -59,42 +65,14 @@ __host__ __device__ inline size_t flat_fixed_bytes( int classes, int attrs, int 
 }
 inline size_t flat_smem_bytes( int classes, int attrs, int tmax )
 {
-	return flat_fixed_bytes( classes, attrs, tmax ) + (size_t)2 * FLAT_MIN_BUF * 16;
+	return flat_fixed_bytes( classes, attrs, tmax ) + (size_t)FLAT_BUFS * FLAT_MIN_BUF * 16;
 }
 
 // ------------------------------------------------------------------------------------
 // building the slices (once per net)
 // ------------------------------------------------------------------------------------
-// 16-byte vectors of a slice of `len` targets: a list of 16-bit indices (dense == 0) or
-// a bitmap of the tile's `words` receiving 32-neuron words (dense == 1, none if len == 0)
-__host__ __device__ inline unsigned slice_vecs( unsigned len, int words, int dense )
-{
-	if( !dense ) return ( len + 7 ) >> 3;
-	return len ? (unsigned)( ( words + 3 ) / 4 ) : 0u;
-}
-
-// lowest and highest tile-local target of every tile over all rows (tiles without
-// inputs keep lo = INT_MAX)
-__global__ void tile_target_range(
-    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first, int * lo, int * hi )
-{
-	long long const total = (long long)n * ntiles;
-	for( long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x )
-	{
-		long long const src = e / ntiles;
-		int const j = (int)( e % ntiles );
-		unsigned const * pv = pivots + src * ( ntiles + 1 ) + j;
-		if( pv[1] > pv[0] )
-		{
-			int const * row = edges + src * width;
-			atomicMin( lo + j, row[pv[0]] - tile_first[j] );
-			atomicMax( hi + j, row[pv[1] - 1] - tile_first[j] );
-		}
-	}
-}
-
 // vectors of every (src, tile) slice, from the ELL pivots, into rec[].x; rec[].y = length
-__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, int2 const * bm_range, int dense, uint2 * rec )
+__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2 * rec )
 {
 	long long const total = (long long)n * ntiles;
 	for( long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x )
@@ -102,7 +80,7 @@ __global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, int2 
 		long long const src = e / ntiles, j = e % ntiles;
 		unsigned const * pv = pivots + src * ( ntiles + 1 ) + j;
 		unsigned const len = pv[1] - pv[0];
-		rec[e] = make_uint2( slice_vecs( len, bm_range[j].y, dense ), len );
+		rec[e] = make_uint2( ( len + 7 ) >> 3, len );
 	}
 }
 
@@ -150,11 +128,10 @@ __global__ void __launch_bounds__( 1024 ) slice_offsets( int n, int ntiles, uint
 	}
 }
 
-// one warp per source row: rebase rec[] to global vector indices and write every slice.
-// Lists: rec.y = length. Bitmaps: rec.y = 1 | class << 1 for a slice with targets, 0 else.
-template <typename Model, bool Dense>
+// one warp per source row: rebase rec[] to global vector indices and write every slice
+template <typename Model>
 __global__ void __launch_bounds__( 256 ) slice_fill(
-    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first, int2 const * bm_range,
+    int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first,
     unsigned long long const * tile_base, uint2 * rec, unsigned short * slices )
 {
 	using N = typename Model::neuron;
@@ -169,32 +146,15 @@ __global__ void __launch_bounds__( 256 ) slice_fill(
 	{
 		uint2 const r = rec[(long long)src * ntiles + j];
 		unsigned long long const first = tile_base[j] + r.x;
-		unsigned const y = Dense ? ( r.y ? 1u | (unsigned)cls << 1 : 0u ) : r.y;
 		__syncwarp();
-		if( lane == 0 ) rec[(long long)src * ntiles + j] = make_uint2( (unsigned)first, y );
+		if( lane == 0 ) rec[(long long)src * ntiles + j] = make_uint2( (unsigned)first, r.y );
 		if( r.y == 0 ) continue;
 		int const d0 = tile_first[j], span = tile_first[j + 1] - d0;
 		unsigned const lo = pv[j];
-		if constexpr( Dense )
-		{
-			unsigned * out = reinterpret_cast<unsigned *>( slices ) + first * 4;
-			int2 const br = bm_range[j];
-			int const padded = (int)slice_vecs( r.y, br.y, 1 ) * 4;
-			for( int e = lane; e < padded; e += 32 ) out[e] = 0u;
-			__syncwarp();
-			for( int e = lane; e < (int)r.y; e += 32 )
-			{
-				int const local = row[lo + e] - d0 - 32 * br.x;
-				atomicOr( out + ( local >> 5 ), 1u << ( local & 31 ) );
-			}
-		}
-		else
-		{
-			unsigned short * out = slices + first * 8;
-			int const padded = (int)( ( r.y + 7 ) & ~7u );
-			for( int e = lane; e < padded; e += 32 )
-				out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
-		}
+		unsigned short * out = slices + first * 8;
+		int const padded = (int)( ( r.y + 7 ) & ~7u );
+		for( int e = lane; e < padded; e += 32 )
+			out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
 	}
 }
 
@@ -327,27 +287,31 @@ __global__ void __launch_bounds__( 256 ) stage_window( net_params p, int L, int 
 // ------------------------------------------------------------------------------------
 // window kernel
 // ------------------------------------------------------------------------------------
-// table[g] = { first vector of the slice, low | vector offset inside its step << 12 } with
-// low = length (lists) or 1 | class << 1 for a bitmap with targets (bitmaps: `wv` vectors
-// each; wv == 0 selects lists)
-__device__ __forceinline__ int ent_low( int2 e ) { return e.y & 0xFFF; }
-__device__ __forceinline__ int ent_vec( int2 e, int wv ) { return wv ? ( ent_low( e ) & 1 ) * wv : ( ent_low( e ) + 7 ) >> 3; }
-__device__ __forceinline__ int ent_cls( int2 e ) { return ( ent_low( e ) >> 1 ) & 7; }
+// table[g] = { first vector of the slice, length | vector offset inside its step << 12 }
+__device__ __forceinline__ int ent_len( int2 e ) { return e.y & 0xFFF; }
+__device__ __forceinline__ int ent_vec( int2 e ) { return ( ent_len( e ) + 7 ) >> 3; }
 __device__ __forceinline__ int ent_off( int2 e ) { return (int)( (unsigned)e.y >> 12 ); }
+
+// how a staged segment runs
+enum seg_mode
+{
+	SEG_PIPE = 0,   // steps [ks, ke) each fit a slice buffer: producers and consumers
+	SEG_PIECES = 1, // step ks alone, its slices in several buffer loads
+	SEG_DIRECT = 2  // step ks alone, counted from the ELL rows (window_counts' path)
+};
 
 __device__ __forceinline__ int stage_arrivals(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int & nent_out, int * scratch );
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int wv );
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int & mode );
 
 // Stage the arrivals of the steps [ks, L) of the window starting at t0, as many whole
-// steps as fit FLAT_ENT_CAP and keep their vector offsets within FLAT_P_BITS. Returns
-// ke: steps [ks, ke) are staged (ke == ks: step ks goes the direct way).
+// steps as fit FLAT_ENT_CAP, and set the segment's mode. Returns the segment's end ke.
 // step_begin[k - ks] = first entry of step k and step_vec[k - ks] = first vector of step
 // k counted from the segment start, for k in [ks, ke].
 __device__ __forceinline__ int stage_table(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int * step_vec,
-    int * scratch, int wv )
+    int * scratch, int bufv, int & mode )
 {
 	constexpr int B = 8; // loads in flight per thread
 	int const tid = threadIdx.x, nt = blockDim.x;
@@ -377,7 +341,12 @@ __device__ __forceinline__ int stage_table(
 	}
 	else
 		ke = stage_arrivals( p, cnts, table, tile, t0, ks, L, step_begin, nent, scratch );
-	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, wv );
+	if( ke == ks )
+	{
+		mode = SEG_DIRECT; // step ks alone exceeds the table
+		return ks + 1;
+	}
+	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, bufv, mode );
 }
 
 // Per-CTA staging (when stage_window did not run or the window did not fit): the
@@ -459,18 +428,20 @@ __device__ __forceinline__ int stage_arrivals(
 	return ke;
 }
 
+
 // Vector offsets of the staged arrivals: prefix over the segment, then relative to each
 // step (table[g].y = length | offset << 12), step_vec[k - ks] = first vector of step k.
-// A step whose vectors do not fit the offset field ends the segment before it; returns
-// the segment's end.
+// The segment ends before the first step whose vectors exceed a slice buffer (`bufv`);
+// if that is step ks, it runs alone: in pieces, or directly if its offsets do not fit
+// FLAT_P_BITS. Returns the segment's end and sets `mode`.
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int wv )
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int & mode )
 {
 	int const tid = threadIdx.x, nt = blockDim.x;
 	int const per = ( nent + nt - 1 ) / nt;
 	int const g0 = min( nent, tid * per ), g1 = min( nent, g0 + per );
 	int run = 0;
-	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g], wv );
+	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g] );
 	int vtotal;
 	int const my_first = block_exclusive_scan( run, scratch, &vtotal );
 	run_first[tid] = my_first;
@@ -483,7 +454,7 @@ __device__ __forceinline__ int stage_offsets(
 		{
 			int const owner = g / per;
 			v = run_first[owner];
-			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h], wv );
+			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h] );
 		}
 		step_vec[k] = v;
 	}
@@ -497,22 +468,27 @@ __device__ __forceinline__ int stage_offsets(
 			while( step_begin[k + 1] <= g ) k++;
 			int2 e = table[g];
 			unsigned const rel = (unsigned)( v - step_vec[k] );
-			int const nv = ent_vec( e, wv );
-			e.y = ent_low( e ) | (int)( ( rel & ( ( 1u << FLAT_P_BITS ) - 1 ) ) << 12 );
+			int const nv = ent_vec( e );
+			e.y = ent_len( e ) | (int)( ( rel & ( ( 1u << FLAT_P_BITS ) - 1 ) ) << 12 );
 			table[g] = e;
 			v += nv;
 		}
 	}
-	// 6. a step whose vectors do not fit the offset field ends the segment before it
 	int kfit = ks;
-	while( kfit < ke && step_vec[kfit + 1 - ks] - step_vec[kfit - ks] < ( 1 << FLAT_P_BITS ) ) kfit++;
+	while( kfit < ke && step_vec[kfit + 1 - ks] - step_vec[kfit - ks] <= bufv ) kfit++;
 	__syncthreads();
-	return kfit;
+	if( kfit > ks )
+	{
+		mode = SEG_PIPE;
+		return kfit;
+	}
+	mode = step_vec[1] - step_vec[0] < ( 1 << FLAT_P_BITS ) ? SEG_PIECES : SEG_DIRECT;
+	return ks + 1;
 }
 
 // one past the last entry of the piece starting at entry `a` of a step whose entries end
 // at `e`: the entries whose vectors fit one buffer of `bufv` vectors together
-__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv, int wv )
+__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv )
 {
 	int const pa = ent_off( table[a] );
 	int lo = a, hi = e; // f(g) = off(g) + vec(g) - pa <= bufv holds for g = a
@@ -520,12 +496,19 @@ __device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int 
 	{
 		int const mid = ( lo + hi ) >> 1;
 		int2 const m = table[mid];
-		if( ent_off( m ) + ent_vec( m, wv ) - pa <= bufv )
+		if( ent_off( m ) + ent_vec( m ) - pa <= bufv )
 			lo = mid;
 		else
 			hi = mid;
 	}
 	return lo + 1;
+}
+
+// vectors of the piece [a, b) of a step whose entries end at e (step_vectors in all)
+__device__ __forceinline__ int piece_vectors( int2 const * table, int a, int b, int e, int step_vectors )
+{
+	if( a >= b ) return 0;
+	return ( b < e ? ent_off( table[b] ) : step_vectors ) - ent_off( table[a] );
 }
 
 __device__ __forceinline__ void cp_async16( void * dst, void const * src )
@@ -535,21 +518,22 @@ __device__ __forceinline__ void cp_async16( void * dst, void const * src )
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wait_group 0;\n" ::: "memory" ); }
+__device__ __forceinline__ void cp_async_wait_but_one() { asm volatile( "cp.async.wait_group 1;\n" ::: "memory" ); }
 
-// copy the slices of entries [a, b) into buf: groups of 8 lanes per entry, lane q copies
-// vectors q, q + 8, ... (a warp instruction touches 4 slices, not 32)
-__device__ __forceinline__ void issue_piece( net_params const & p, int2 const * table, int a, int b, uint4 * buf, int wv )
+// copy the slices of entries [a, b) into buf, by threads [0, nthreads) of the caller's
+// numbering `t`: groups of 4 lanes per entry, lane q copies vectors q, q + 4, ...
+__device__ __forceinline__ void issue_piece( net_params const & p, int2 const * table, int a, int b, uint4 * buf, int t, int nthreads )
 {
 	if( a >= b ) return;
 	int const pa = ent_off( table[a] );
-	int const q = threadIdx.x & 7, groups = blockDim.x >> 3;
-	for( int g = a + (int)( threadIdx.x >> 3 ); g < b; g += groups )
+	int const q = t & 3, groups = nthreads >> 2;
+	for( int g = a + ( t >> 2 ); g < b; g += groups )
 	{
 		int2 const e = table[g];
-		int const nv = ent_vec( e, wv );
+		int const nv = ent_vec( e );
 		uint4 const * src = p.slices + (unsigned)e.x;
 		uint4 * dst = buf + ( ent_off( e ) - pa );
-		for( int j = q; j < nv; j += 8 ) cp_async16( dst + j, src + j );
+		for( int j = q; j < nv; j += 4 ) cp_async16( dst + j, src + j );
 	}
 }
 
@@ -558,11 +542,11 @@ __device__ __forceinline__ void count_index( unsigned * cnt, unsigned x )
 	if( x != SLICE_PAD ) atomicAdd( cnt + x, 1u );
 }
 
-// count every index of the `V` vectors in buf
-__device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned * cnt )
+// count every index of the `V` vectors in buf, by threads [0, nthreads) of numbering `t`
+__device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned * cnt, int t, int nthreads )
 {
 #pragma unroll 2
-	for( int v = threadIdx.x; v < V; v += blockDim.x )
+	for( int v = t; v < V; v += nthreads )
 	{
 		uint4 const w = buf[v];
 		count_index( cnt, w.x & 0xFFFFu );
@@ -576,79 +560,32 @@ __device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned
 	}
 }
 
-// vectors of the piece [a, b) of a step whose entries end at e (step_vectors in all)
-__device__ __forceinline__ int piece_vectors( int2 const * table, int a, int b, int e, int step_vectors )
-{
-	if( a >= b ) return 0;
-	return ( b < e ? ent_off( table[b] ) : step_vectors ) - ent_off( table[a] );
-}
+// barrier of the first `threads` threads (whole warps) of the CTA
+__device__ __forceinline__ void bar_sync_first( int threads ) { asm volatile( "bar.sync 1, %0;\n" ::"r"( threads ) : "memory" ); }
 
-// 32 x 32 bit transpose across a warp: afterwards bit j of lane l is bit l of lane j
-__device__ __forceinline__ unsigned warp_transpose32( unsigned x, int lane )
+// ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
+// per round, a warp scan of their counts gives every word's offset
+__device__ __forceinline__ void compact_step( net_params const & p, unsigned const * bits, int words, int d0, int tile, long long t, int lane )
 {
-#pragma unroll
-	for( int s = 16; s >= 1; s >>= 1 )
+	int const slot_out = (int)( t % p.ring );
+	int * out = p.ring_ids + (long long)slot_out * p.n + d0;
+	int done = 0;
+	for( int w0 = 0; w0 < words; w0 += 32 )
 	{
-		unsigned const m = s == 16 ? 0x0000FFFFu : s == 8 ? 0x00FF00FFu : s == 4 ? 0x0F0F0F0Fu : s == 2 ? 0x33333333u : 0x55555555u;
-		unsigned const y = __shfl_xor_sync( 0xffffffffu, x, s );
-		// lanes with bit s set keep their high halves and take the partner's high halves
-		// shifted down, the others keep their low halves and take the partner's low halves
-		// shifted up (~m >> s == m for these masks)
-		bool const up = lane & s;
-		unsigned const keep = up ? ~m : m;
-		unsigned const z = up ? y >> s : y << s;
-		x = ( x & keep ) | ( z & ~keep );
+		int const w = w0 + lane;
+		unsigned m = w < words ? bits[w] : 0u;
+		int const c = __popc( m );
+		int const incl = warp_inclusive_scan( c );
+		int off = done + incl - c;
+		while( m )
+		{
+			int const b = __ffs( m ) - 1;
+			m &= m - 1;
+			out[off++] = d0 + ( w << 5 ) + b;
+		}
+		done += __shfl_sync( 0xffffffffu, incl, 31 );
 	}
-	return x;
-}
-
-// Bitmap counting. Slots [s0, s1) lie in `buf` from slot `base` on, `ww` words each. For
-// bitmap word w, lane l adds the words of slots s0 + l, s0 + l + 32, ... into four bit
-// planes (a per-bit counter up to 15), in rounds of 15 slots per lane; transposing a plane
-// makes lane l's popcount the number of planes' bits l over all lanes. Returns this lane's
-// count for bit `lane` of word w.
-__device__ __forceinline__ unsigned bitmap_count( unsigned const * buf, int base, int s0, int s1, int ww, int w, int lane )
-{
-	unsigned total = 0;
-	for( int r0 = s0; r0 < s1; r0 += 15 * 32 )
-	{
-		int const r1 = min( s1, r0 + 15 * 32 );
-		unsigned p0 = 0, p1 = 0, p2 = 0, p3 = 0;
-		for( int s = r0 + lane; s < r1; s += 32 )
-		{
-			unsigned c = buf[( s - base ) * ww + w];
-			unsigned t = p0 & c;
-			p0 ^= c;
-			c = t;
-			t = p1 & c;
-			p1 ^= c;
-			c = t;
-			t = p2 & c;
-			p2 ^= c;
-			p3 ^= t; // no carry out: a lane adds at most 15 words
-		}
-		// planes needed for the largest lane count (uniform across the warp)
-		int const most = ( r1 - r0 + 31 ) >> 5;
-		if( most >= 8 )
-		{
-			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane ), c = warp_transpose32( p2, lane ),
-			               d = warp_transpose32( p3, lane );
-			total += __popc( a ) + ( __popc( b ) << 1 ) + ( __popc( c ) << 2 ) + ( __popc( d ) << 3 );
-		}
-		else if( most >= 4 )
-		{
-			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane ), c = warp_transpose32( p2, lane );
-			total += __popc( a ) + ( __popc( b ) << 1 ) + ( __popc( c ) << 2 );
-		}
-		else if( most >= 2 )
-		{
-			unsigned const a = warp_transpose32( p0, lane ), b = warp_transpose32( p1, lane );
-			total += __popc( a ) + ( __popc( b ) << 1 );
-		}
-		else
-			total += __popc( warp_transpose32( p0, lane ) );
-	}
-	return total;
+	if( lane == 0 ) p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
 }
 
 // neuron state of the tile: shared memory [attrs][span] <-> registers / global memory
@@ -711,14 +648,13 @@ struct smem_state
 	}
 };
 
-template <typename Model, bool Dense>
+template <typename Model>
 __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
 {
 	using N = typename Model::neuron;
 	using Tup = typename N::template apply<reg_tuple>;
 	constexpr int C = N::input_classes;
 	static_assert( C >= 1, "window_flat needs a model with input classes" );
-	static_assert( !Dense || C <= 4, "bitmap slices carry up to four input classes" );
 
 	extern __shared__ __align__( 128 ) unsigned char smem[];
 	__shared__ int scratch[33];
@@ -727,15 +663,11 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	__shared__ float s_c, s_sum;
 	__shared__ int step_begin[MAX_WINDOW + 1];
 	__shared__ int step_vec[MAX_WINDOW + 1];
-	__shared__ int s_cslots[MAX_WINDOW][4]; // bitmaps: slots of every input class per step
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+	int const nwc = nw - FLAT_PRODUCERS, ncons = nwc * 32; // consumer warps first, then producers
 	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
-	// bitmaps: words [bw0, bw0 + bwn) of the tile hold all its targets, wv vectors each
-	int2 const brange = Dense ? __ldg( p.bm_range + tile ) : make_int2( 0, 0 );
-	int const bw0 = brange.x, bwn = brange.y;
-	int const wv = Dense ? max( 1, ( bwn + 3 ) >> 2 ) : 0;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
 	snn_info const info{ p.n };
 
@@ -745,220 +677,162 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	size_t const fixed = flat_fixed_bytes( C, (int)N::size, span );
 	int2 * table = reinterpret_cast<int2 *>( smem + fixed - (size_t)FLAT_ENT_CAP * 8 - (size_t)FLAT_SCRATCH * 4 );
 	unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
-	int const bufv = (int)( ( (size_t)smem_bytes - fixed ) / 32 );
-	uint4 * const buf0 = reinterpret_cast<uint4 *>( smem + fixed );
-	uint4 * const buf1 = buf0 + bufv;
+	int const bufv = inputs ? (int)( ( (size_t)smem_bytes - fixed ) / ( 16 * FLAT_BUFS ) ) : 0;
+	uint4 * const buf0 = reinterpret_cast<uint4 *>( smem + fixed ); // FLAT_BUFS buffers of bufv vectors
 
 	window_clock_begin( p, L, dt, s_dt, &s_t0, &s_c, &s_sum );
 	long long const t0 = s_t0;
 	smem_state<N>::from_global( p.attr, d0, span, state );
-	// counters start at zero; the update phase zeroes every counter it consumes
+	// counters start at zero; the update zeroes every counter it consumes
 	if( inputs )
 		for( int x = tid; x < C * span; x += nt ) cnt[x] = 0;
 	__syncthreads();
 
-	int ks = 0;
-	while( ks < L )
+	// update of step k by warps [0, nws): warp w owns neurons [32 w, 32 w + 32) + 32 nws r,
+	// one fired-bit word each (bits of step k in half k & 1)
+	auto update = [&]( int k, int nws ) {
+		long long const t = t0 + k;
+		bool const arrivals = inputs && t >= p.delay;
+		unsigned * bits = bits2 + ( k & 1 ) * words;
+		for( int base = warp * 32; base < span; base += nws * 32 )
+		{
+			int const local = base + lane;
+			bool fired = false;
+			if( local < span )
+			{
+				Tup st;
+				smem_state<N>::load( st, state, span, local );
+				uint32_t const i = (uint32_t)( d0 + local );
+				reg_iter<Tup> it{ st, i };
+				if( arrivals )
+#pragma unroll
+					for( int c = 0; c < C; c++ )
+					{
+						unsigned const m = cnt[c * span + local];
+						if( m )
+						{
+							cnt[c * span + local] = 0u;
+							repeat_backend rb( p.seed, i, (uint32_t)t, m );
+							N::receive( N::class_source( c, info ), it, null_syn_iter{}, info, rb );
+						}
+					}
+				device_backend bak( p.seed, i, (uint32_t)t );
+				fired = N::update( it, s_dt[k], info, bak );
+				smem_state<N>::store( st, state, span, local );
+			}
+			unsigned const word = __ballot_sync( 0xffffffffu, fired );
+			if( lane == 0 ) bits[base >> 5] = word;
+		}
+	};
+	auto compact = [&]( int k ) { compact_step( p, bits2 + ( k & 1 ) * words, words, d0, tile, t0 + k, lane ); };
+
+	if( !inputs )
 	{
-		int const ke = inputs ? stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch, wv ) : L;
-		bool const direct = ke == ks; // step ks alone exceeds the table
-		int const kend = direct ? ks + 1 : ke;
-		bool const piped = inputs && !direct; // slices flow through the two buffers
-		if( Dense && piped )
+		// no arrivals: every warp updates, the last warp compacts the step before while the
+		// others update the next one (its bits are in the other half)
+		for( int k = 0; k < L; k++ )
 		{
-			// bitmaps of every input class per step (slots ascend with the source id, and so
-			// does the class)
-			for( int x = tid; x < ( kend - ks ) * 4; x += nt ) s_cslots[x >> 2][x & 3] = 0;
+			update( k, nw );
 			__syncthreads();
-			int const nent = step_begin[kend - ks];
-			for( int g = tid; g < nent; g += nt )
+			if( warp == nw - 1 ) compact( k );
+		}
+		__syncthreads();
+	}
+	else
+	{
+		int ks = 0;
+		while( ks < L )
+		{
+			int mode;
+			int const ke = stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch, bufv, mode );
+			if( mode == SEG_PIPE )
 			{
-				int2 const e = table[g];
-				if( ent_low( e ) & 1 )
+				// producers copy step k + 2 while consumers count and update step k
+				int const pt = tid - ncons, npt = nt - ncons;
+				auto issue_step = [&]( int k ) {
+					issue_piece( p, table, step_begin[k - ks], step_begin[k + 1 - ks], buf0 + ( k % FLAT_BUFS ) * bufv, pt, npt );
+					cp_async_commit();
+				};
+				if( warp >= nwc )
 				{
-					int lo = 0, hi = kend - ks; // step of g: last k with step_begin[k] <= g
-					while( hi - lo > 1 )
+					issue_step( ks );
+					if( ks + 1 < ke )
 					{
-						int const mid = ( lo + hi ) >> 1;
-						if( step_begin[mid] <= g )
-							lo = mid;
-						else
-							hi = mid;
+						issue_step( ks + 1 );
+						cp_async_wait_but_one();
 					}
-					atomicAdd( &s_cslots[lo][ent_cls( e )], 1 );
-				}
-			}
-			__syncthreads();
-		}
-
-		// first piece [a, b) of step k
-		auto first_piece = [&]( int k, int & a, int & b ) {
-			a = step_begin[k - ks];
-			int const e = step_begin[k + 1 - ks];
-			b = a < e ? piece_end( table, a, e, bufv, wv ) : a;
-		};
-		if( piped )
-		{
-			// the first pieces of steps ks and ks + 1 in flight before the loop
-			for( int k = ks; k < min( ks + 2, kend ); k++ )
-			{
-				int a, b;
-				first_piece( k, a, b );
-				issue_piece( p, table, a, b, ( k & 1 ) ? buf1 : buf0, wv );
-			}
-			cp_async_commit();
-			cp_async_wait_all();
-			__syncthreads();
-		}
-
-		for( int k = ks; k < kend; k++ )
-		{
-			long long const t = t0 + k;
-			bool const arrivals = t >= p.delay;
-			uint4 * const bk = ( k & 1 ) ? buf1 : buf0;
-			if( inputs && arrivals )
-			{
-				if( direct )
-				{
-					// the direct path of window_counts, its scratch in the (unused) table
-					int * pref = reinterpret_cast<int *>( table );
-					int4 * sb = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( table ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
-					net_params q = p;
-					q.tile = span; // counter rows are span long
-					deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sb, scratch );
-				}
-				else
-				{
-					int const e = step_begin[k + 1 - ks];
-					int const sv = step_vec[k + 1 - ks] - step_vec[k - ks];
-					// bitmaps: the warp that owns word w counts it for all classes; the
-					// counts land in the counter rows the update reads
-					auto count_piece = [&]( int a, int b ) {
-						if constexpr( Dense )
-						{
-							if( a >= b ) return;
-							int const slot0 = ent_off( table[a] ) / wv;
-							int const slot1 = ( b < e ? ent_off( table[b] ) : sv ) / wv;
-							unsigned const * bw = reinterpret_cast<unsigned const *>( bk );
-							// class 0 = all slots minus the other classes (fewer planes to move).
-							// Warp `warp` counts the tile words it updates below (warp + r nw),
-							// so no barrier is needed between counting and the update.
-							for( int tw = warp; tw < bw0 + bwn; tw += nw )
-							{
-								if( tw < bw0 ) continue;
-								int const w = tw - bw0;
-								int const local = ( tw << 5 ) + lane;
-								unsigned rest = 0;
-								int c0 = s_cslots[k - ks][0];
-#pragma unroll
-								for( int c = 1; c < C; c++ )
-								{
-									int const c1 = c0 + s_cslots[k - ks][c];
-									int const lo = max( c0, slot0 ), hi = min( c1, slot1 );
-									if( lo < hi )
-									{
-										unsigned const m = bitmap_count( bw, slot0, lo, hi, wv * 4, w, lane );
-										if( local < span ) cnt[c * span + local] += m;
-										rest += m;
-									}
-									c0 = c1;
-								}
-								unsigned const all = bitmap_count( bw, slot0, slot0, slot1, wv * 4, w, lane );
-								if( local < span ) cnt[local] += all - rest;
-							}
-						}
-						else
-							count_buffer( bk, piece_vectors( table, a, b, e, sv ), cnt );
-					};
-					int a, b;
-					first_piece( k, a, b );
-					count_piece( a, b );
-					while( b < e ) // the rest of a step larger than a buffer
-					{
-						__syncthreads(); // bk is free
-						a = b;
-						b = piece_end( table, a, e, bufv, wv );
-						issue_piece( p, table, a, b, bk, wv );
-						cp_async_commit();
+					else
 						cp_async_wait_all();
-						__syncthreads();
-						count_piece( a, b );
-					}
 				}
-			}
-			// counts complete (bitmaps: every warp counted its own words, no barrier needed)
-			if( !Dense || !piped ) __syncthreads();
-			unsigned * bits = bits2 + ( k & 1 ) * words; // the compaction of step k - 1 reads the other half
-
-			// update: warp w owns neurons [32 w, 32 w + 32) + 32 nw * round; one bit word each
-			for( int base = warp * 32; base < span; base += nw * 32 )
-			{
-				int const local = base + lane;
-				bool fired = false;
-				if( local < span )
+				__syncthreads();
+				for( int k = ks; k < ke; k++ )
 				{
-					Tup st;
-					smem_state<N>::load( st, state, span, local );
-					uint32_t const i = (uint32_t)( d0 + local );
-					reg_iter<Tup> it{ st, i };
-					if( inputs && arrivals )
-#pragma unroll
-						for( int c = 0; c < C; c++ )
-						{
-							unsigned const m = cnt[c * span + local];
-							if( m )
-							{
-								cnt[c * span + local] = 0u;
-								repeat_backend rb( p.seed, i, (uint32_t)t, m );
-								N::receive( N::class_source( c, info ), it, null_syn_iter{}, info, rb );
-							}
-						}
-					device_backend bak( p.seed, i, (uint32_t)t );
-					fired = N::update( it, s_dt[k], info, bak );
-					smem_state<N>::store( st, state, span, local );
-				}
-				unsigned const word = __ballot_sync( 0xffffffffu, fired );
-				if( lane == 0 ) bits[base >> 5] = word;
-			}
-			if( piped ) cp_async_wait_all(); // this thread's copies for step k + 1
-			__syncthreads();                 // fired bits and step k + 1's slices complete
-			if( piped && k + 2 < kend )
-			{
-				// step k + 2 into the buffer step k was counted from (done: barrier above)
-				int a, b;
-				first_piece( k + 2, a, b );
-				issue_piece( p, table, a, b, bk, wv );
-				cp_async_commit();
-			}
-			// ascending compaction by the last warp, without a further barrier: 32 words per
-			// round, a warp scan of their counts gives every word's offset. The other warps
-			// go on to the next step's counting; bits are rewritten only after the next
-			// step's first barrier, and counters were zeroed where they were consumed.
-			if( warp == nw - 1 )
-			{
-				int const slot_out = (int)( t % p.ring );
-				int * out = p.ring_ids + (long long)slot_out * p.n + d0;
-				int done = 0;
-				for( int w0 = 0; w0 < words; w0 += 32 )
-				{
-					int const w = w0 + lane;
-					unsigned m = w < words ? bits[w] : 0u;
-					int const c = __popc( m );
-					int const incl = warp_inclusive_scan( c );
-					int off = done + incl - c;
-					while( m )
+					if( warp < nwc )
 					{
-						int const b = __ffs( m ) - 1;
-						m &= m - 1;
-						out[off++] = d0 + ( w << 5 ) + b;
+						if( t0 + k >= p.delay )
+							count_buffer( buf0 + ( k % FLAT_BUFS ) * bufv, step_vec[k + 1 - ks] - step_vec[k - ks], cnt, tid, ncons );
+						bar_sync_first( ncons ); // counts complete
+						update( k, nwc );
 					}
-					done += __shfl_sync( 0xffffffffu, incl, 31 );
+					else
+					{
+						// the buffer of step k + 2 was last read by step k - 1's counting
+						if( k + 2 < ke )
+						{
+							issue_step( k + 2 );
+							cp_async_wait_but_one(); // step k + 1's copies are complete
+						}
+						else
+							cp_async_wait_all();
+						if( k > ks && warp == nw - 1 ) compact( k - 1 );
+					}
+					__syncthreads(); // step k updated, step k + 1's slices in place
 				}
-				if( lane == 0 ) p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
+				if( warp == nw - 1 ) compact( ke - 1 );
+				__syncthreads();
 			}
+			else
+			{
+				// step ks alone, every warp
+				int const k = ks;
+				long long const t = t0 + k;
+				if( t >= p.delay )
+				{
+					if( mode == SEG_DIRECT )
+					{
+						// the direct path of window_counts, its scratch in the (unused) table
+						int * pref = reinterpret_cast<int *>( table );
+						int4 * sb = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( table ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
+						net_params q = p;
+						q.tile = span; // counter rows are span long
+						deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sb, scratch );
+					}
+					else
+					{
+						// pieces that fit all the slice buffers together
+						int const e = step_begin[1];
+						int const sv = step_vec[1] - step_vec[0];
+						for( int a = 0, b = 0; b < e; )
+						{
+							a = b;
+							b = piece_end( table, a, e, FLAT_BUFS * bufv );
+							issue_piece( p, table, a, b, buf0, tid, nt );
+							cp_async_commit();
+							cp_async_wait_all();
+							__syncthreads();
+							count_buffer( buf0, piece_vectors( table, a, b, e, sv ), cnt, tid, nt );
+							__syncthreads();
+						}
+					}
+				}
+				__syncthreads();
+				update( k, nw );
+				__syncthreads();
+				if( warp == nw - 1 ) compact( k );
+				__syncthreads();
+			}
+			ks = ke;
 		}
-		ks = kend;
-		__syncthreads(); // compaction reads of bits are done before the next segment or the exit
 	}
 
 	smem_state<N>::to_global( p.attr, d0, span, state );

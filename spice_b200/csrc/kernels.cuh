@@ -65,7 +65,6 @@ struct net_params
 	uint4 const * slices;    // tile-major 16-bit slices (window_flat)
 	uint2 const * slice_rec; // [n][ntiles] { first vector, length } (window_flat)
 	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
-	int2 const * bm_range;   // [ntiles] { first word, words } of the tile's bitmaps (window_flat)
 	uint2 * wtab;            // [ntiles][ecap] the window's arrivals per tile (stage_window)
 	int * wsteps;            // [MAX_WINDOW + 2] first arrival of every step, validity flag
 	int ecap;                // arrivals per window wtab holds (0: no stage_window)

@@ -232,10 +232,8 @@ struct spk_net
 	bool flat = false;
 	int flat_tmax = 0;   // the largest tile of the flat tiling
 	int flat_smem = 0;   // dynamic shared memory of a window_flat launch
-	bool dense = false;  // slices are tile bitmaps (else 16-bit index lists)
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
-	dbuf bm_range;          // [ntiles] receiving word range of every tile (bitmaps)
 	dbuf wtab, wsteps;      // per-window arrival tables of stage_window
 	int ecap = 0;           // arrivals per window stage_window handles (0: off)
 	int stage_chunk = 0;    // arrivals a stage_window CTA transposes at once
@@ -269,7 +267,6 @@ struct spk_net
 		p.slices = slices.as<uint4 const>();
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
-		p.bm_range = bm_range.as<int2 const>();
 		p.wtab = wtab.as<uint2>();
 		p.wsteps = wsteps.as<int>();
 		p.ecap = ecap;
@@ -280,8 +277,7 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + bm_range.bytes + wtab.bytes +
-		           wsteps.bytes;
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + wtab.bytes + wsteps.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -335,18 +331,11 @@ struct spk_net
 				// becomes slice buffers
 				int optin = 0;
 				CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
-				cudaFuncAttributes fa{}, fb{};
-				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model, false> ) );
+				cudaFuncAttributes fa{};
+				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model> ) );
 				flat_smem = optin - (int)fa.sharedSizeBytes;
-				if constexpr( Model::neuron::input_classes <= 4 )
-				{
-					CK( cudaFuncGetAttributes( &fb, spk::window_flat<Model, true> ) );
-					flat_smem = std::min( flat_smem, optin - (int)fb.sharedSizeBytes );
-				}
 				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
-				CK( cudaFuncSetAttribute( spk::window_flat<Model, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
-				if constexpr( Model::neuron::input_classes <= 4 )
-					CK( cudaFuncSetAttribute( spk::window_flat<Model, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
 				return;
 			}
 		with_window_kernel<Model>( [&]( auto kernel ) {
@@ -382,14 +371,7 @@ struct spk_net
 				spk::stage_window<<<2 * sms, 256, spk::stage_window_smem( tc.ntiles, stage_chunk ), stream>>>( p, L, stage_chunk );
 				CK( cudaGetLastError() );
 			}
-			if constexpr( Model::neuron::input_classes <= 4 )
-				if( dense )
-				{
-					spk::window_flat<Model, true><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
-					CK( cudaGetLastError() );
-					return;
-				}
-			spk::window_flat<Model, false><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
 		}
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
@@ -723,15 +705,9 @@ void fill_slices( spk_net & net, dbuf const & bases )
 	if constexpr( Model::neuron::input_classes > 0 )
 	{
 		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
-		auto fill = [&]( auto kernel ) {
-			kernel<<<blocks, 256, 0, net.stream>>>(
-			    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
-			    net.bm_range.as<int2>(), bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
-		};
-		if( net.dense )
-			fill( spk::slice_fill<Model, true> );
-		else
-			fill( spk::slice_fill<Model, false> );
+		spk::slice_fill<Model><<<blocks, 256, 0, net.stream>>>(
+		    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
+		    bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
 		CK( cudaGetLastError() );
 	}
 }
@@ -745,54 +721,13 @@ void build_slices( spk_net & net )
 	totals.alloc( (size_t)nt * 8 );
 	bases.alloc( (size_t)nt * 8 );
 	std::vector<unsigned long long> tot( nt ), base( nt );
-	// receiving word range of every tile: bitmaps cover only these words
-	{
-		dbuf lo, hi;
-		lo.alloc( (size_t)nt * 4 );
-		hi.alloc( (size_t)nt * 4 );
-		std::vector<int> l( nt, INT_MAX ), h( nt, -1 );
-		CK( cudaMemcpyAsync( lo.p, l.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
-		CK( cudaMemcpyAsync( hi.p, h.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
-		if( net.width > 0 )
-		{
-			spk::tile_target_range<<<4 * net.sms, 256, 0, net.stream>>>(
-			    (int)net.n, (int)net.width, nt, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(), lo.as<int>(), hi.as<int>() );
-			CK( cudaGetLastError() );
-		}
-		CK( cudaMemcpyAsync( l.data(), lo.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
-		CK( cudaMemcpyAsync( h.data(), hi.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
-		CK( cudaStreamSynchronize( net.stream ) );
-		std::vector<int2> r( nt );
-		for( int j = 0; j < nt; j++ ) r[j] = h[j] < 0 ? make_int2( 0, 0 ) : make_int2( l[j] / 32, h[j] / 32 - l[j] / 32 + 1 );
-		net.bm_range.alloc( (size_t)nt * sizeof( int2 ) );
-		CK( cudaMemcpyAsync( net.bm_range.p, r.data(), (size_t)nt * sizeof( int2 ), cudaMemcpyHostToDevice, net.stream ) );
-		CK( cudaStreamSynchronize( net.stream ) );
-	}
-	// vectors per (src, tile) and their per-tile prefix, as lists or as bitmaps
-	auto layout_pass = [&]( int dense ) {
-		spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>(
-		    (int)net.n, nt, net.pivots.as<unsigned>(), net.bm_range.as<int2>(), dense, net.slice_rec.as<uint2>() );
-		CK( cudaGetLastError() );
-		spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
-		CK( cudaGetLastError() );
-		CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
-		CK( cudaStreamSynchronize( net.stream ) );
-		unsigned long long all = 0;
-		for( auto v : tot ) all += v;
-		return all;
-	};
-	// bitmaps where they take fewer bytes than index lists (dense connectivity, p > ~1/16),
-	// SPK_SLICES=list|bitmap forces one
-	char const * mode = getenv( "SPK_SLICES" );
-	bool const can_dense = net.classes() <= 4;
-	unsigned long long const list_vecs = layout_pass( 0 );
-	net.dense = false;
-	if( can_dense && !( mode && !strcmp( mode, "list" ) ) )
-	{
-		unsigned long long const dense_vecs = layout_pass( 1 );
-		net.dense = dense_vecs <= list_vecs || ( mode && !strcmp( mode, "bitmap" ) );
-		if( !net.dense ) layout_pass( 0 );
-	}
+	// vectors per (src, tile) and their per-tile prefix
+	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>() );
+	CK( cudaGetLastError() );
+	spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
+	CK( cudaGetLastError() );
+	CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
+	CK( cudaStreamSynchronize( net.stream ) );
 	unsigned long long all = 0;
 	for( int j = 0; j < nt; j++ )
 	{

@@ -131,16 +131,7 @@ def run_parity(model, pops, conns, delay, steps, seed, edges=None, width=None, g
     return net, ref
 
 
-@pytest.fixture(params=["auto", "list", "bitmap"])
-def slices(request):
-    """window_flat's slice layout: chosen by size, or forced to 16-bit lists or bitmaps."""
-    if request.param != "auto":
-        os.environ["SPK_SLICES"] = request.param
-    yield request.param
-    os.environ.pop("SPK_SLICES", None)
-
-
-def test_va_step_from_cpu_net(slices):
+def test_va_step_from_cpu_net():
     # spice_test/cuda/snn.d.cpp:104-139 (N = 4000, p = 0.02, 1000 steps)
     ref = oracle.OracleNet("vogels_abbott", [4000], [(0, 0, 0.02)], delay=1, graph="reference", graph_seed=1337)
     e, w = ref.adj()
@@ -155,7 +146,7 @@ def test_va_step_with_delay():
 
 
 @pytest.mark.parametrize("name", ["va_n1000_d1", "va_n1000_d8", "brunel_n1000_d15", "brunelp_n600_d15"])
-def test_against_reference_golden(name, slices):
+def test_against_reference_golden(name):
     g = golden(name)
     w = int(g["width"])
     edges = ell(g["lens"], g["ids"], w)
@@ -179,11 +170,11 @@ def test_against_reference_golden(name, slices):
 
 
 @pytest.mark.parametrize("delay", [1, 3, 15])
-def test_brunel_generated_graph(delay, slices):
+def test_brunel_generated_graph(delay):
     run_parity("brunel", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], delay, 1000, 5, graph_seed=21)
 
 
-def test_synth_model(slices):
+def test_synth_model():
     run_parity("synth", [3000], [(0, 0, 0.01)], 4, 300, 9, graph_seed=3)
 
 
@@ -257,16 +248,15 @@ def test_errors():
     (400_000, 15, 60, None, 16),     # ~2000 per step: more than stage_window holds, per-CTA staging
     (150_000, 15, 60, "cta", 16),    # per-CTA staging throughout
     (1_700_000, 4, 24, None, 16),    # > 8192 arrivals in one step: the direct path inside window_flat
-    (150_000, 15, 60, "bitmap", 16), # bitmaps of 1 k-neuron tiles
-    (400_000, 8, 32, "bitmap", 800), # bitmaps larger than a buffer: several pieces per step
-    (400_000, 8, 32, "bitmap+uniform", 800),  # 1 k-neuron tiles, ~2000 bitmaps per piece: counting rounds
+    (1_000_000, 4, 16, None, 800),   # ~5000 slices per tile and step: more than a buffer, in pieces
+    (400_000, 8, 32, "uniform", 800),  # equal 1 k-neuron tiles
 ])
 def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage, deg):
     """window_flat (staged table, balanced tiles, slice buffers) against window_counts,
     itself checked against the oracle above, on nets too large for the oracle to step
     quickly."""
     layout = Layout(n, deg / n)
-    env = {"cta": ("SPK_STAGE", "cta"), "bitmap": ("SPK_SLICES", "bitmap"), "uniform": ("SPK_TILES", "uniform")}
+    env = {"cta": ("SPK_STAGE", "cta"), "uniform": ("SPK_TILES", "uniform")}
     for f in (stage.split("+") if stage else []):
         os.environ[env[f][0]] = env[f][1]
     try:
