@@ -10,28 +10,29 @@
 // CTA reads only its own tile's region, two bytes per synapse, already in the form its
 // counters are indexed by.
 //
-//   1. Staging. All arrivals of the window fired before it started: stage_window (or the
-//      CTA itself) builds the window's arrival table (first vector, length, vector offset
-//      inside the step) in shared memory.
-//   2. Producers. FLAT_PRODUCERS warps copy the slices of step k + 2 into one of three
-//      shared-memory buffers with cp.async while the other warps work on step k, so the
-//      burst of scattered loads that every tile issues at the same time overlaps counting
-//      and updating instead of stalling them.
-//   3. Consumers count step k from its buffer, one 16-byte vector per thread at a time,
-//      with a shared-memory atomic per index; a consumer-only barrier; then they replay
-//      the counts through the model's receive(), update every neuron and zero the
-//      counters they consumed. The tile's neuron state stays in shared memory for the
-//      whole window.
-//   4. A producer warp compacts the fired neurons of step k - 1 in ascending order into
-//      the spike ring. One block-wide barrier per step.
-// A step whose slices exceed a buffer, or whose arrivals exceed the table, runs alone with
-// every warp (pieces loaded synchronously, or the direct path of window_counts).
+// All arrivals of a window fired before it started, so a step's arrivals can be prepared
+// steps ahead. The CTA splits into FLAT_PRODUCERS producer warps and consumer warps. While
+// the consumers work on step k, the producers
+//   - copy the slices of step k + 1 into a shared-memory ring with cp.async,
+//   - load the slice records of step k + 2's arrivals and lay out their ring offsets,
+//   - load the spike ids of step k + 3 (the per-source-tile spike counts, scanned),
+//   - load the per-source-tile spike counts of step k + 4,
+//   - and compact the fired neurons of step k - 1 in ascending order into the spike ring,
+// each stage one global-memory round trip that a whole step hides. The consumers count
+// step k from the ring, one 16-byte vector per thread at a time with a shared-memory
+// atomic per index; a consumer-only barrier; then they replay the counts through the
+// model's receive(), update every neuron and zero the counters they consumed. The tile's
+// neuron state stays in shared memory for the whole window; one block-wide barrier per
+// step. A step with more arrivals than a step table holds, or more slices than the ring,
+// switches the rest of the window to a synchronous path (window-wide staging, slices in
+// pieces or the direct path of window_counts).
 // Keeping the state in shared memory lets tile sizes follow the work (balanced tiles): a
 // population without inputs costs little per neuron and gets few, large tiles.
 //
 // Measured on B200 (Brunel, 1e9 synapses): scattered 16-byte copies issue at about one per
 // cycle per SM, and since all tiles issue theirs at the same moment the burst runs near
-// HBM bandwidth; issued by the warps that then count, it sat on every step's critical path.
+// HBM bandwidth; issued by the warps that then count, it sat on every step's critical
+// path, and staging a whole window before its first step cost more than the steps.
 #pragma once
 
 #include "kernels.cuh"
@@ -39,20 +40,22 @@
 namespace spk
 {
 constexpr int FLAT_THREADS = 1024;    // threads of a window_flat CTA (one CTA per SM)
-constexpr int FLAT_PRODUCERS = 8;     // warps that copy slices and compact spikes
-constexpr int FLAT_BUFS = 3;          // slice buffers: step k counted, k + 1 ready, k + 2 loading
-constexpr int FLAT_ENT_CAP = 6144;    // staged arrivals per segment of a window
-constexpr int FLAT_SCRATCH = 2560;    // per-(step, source tile) counts staged at once (>= threads)
+constexpr int FLAT_PRODUCERS = 8;     // warps that stage, copy slices and compact spikes
+constexpr int FLAT_PC = 1032;         // per-source-tile counts of one step (ntiles + 1 <= FLAT_PC)
+constexpr int FLAT_STEP_CAP = 1024;   // arrivals of one step the pipeline stages
+constexpr int FLAT_ENT_CAP = 6144;    // arrivals per segment of the synchronous path
+constexpr int FLAT_SCRATCH = 2560;    // per-(step, source tile) counts it stages at once (>= threads)
 constexpr int FLAT_MAX_TILE = 4064;   // slice lengths fit the table's 12-bit field
 constexpr int FLAT_MIN_BUF = 512;     // vectors per buffer at least (one slice of a full tile)
 constexpr int FLAT_P_BITS = 20;       // vector offsets inside a step held in the table
-constexpr int FLAT_STAGE_CAP = 16384; // arrivals per window stage_window stages
 constexpr unsigned short SLICE_PAD = 0xFFFFu;
 static_assert( FLAT_SCRATCH >= FLAT_THREADS, "staging keeps one prefix per thread in the scratch" );
+static_assert( FLAT_STEP_CAP <= ( 1 << FLAT_P_BITS ), "step offsets fit the table" );
 
 // shared memory of a CTA: neuron state [attrs][span], fired bits [2][words]; tiles with
-// inputs add counters [classes][span], the arrival table, staging scratch and FLAT_BUFS
-// slice buffers in what is left
+// inputs add counters [classes][span], the per-step staging ring (counts [4][FLAT_PC],
+// tables [4][FLAT_STEP_CAP]) and the slice ring in what is left (the synchronous path
+// keeps its table, scratch and buffer there)
 __host__ __device__ inline size_t flat_state_bytes( int attrs, int span )
 {
 	return (size_t)attrs * span * 4 + 2 * ( ( (size_t)span + 31 ) / 32 ) * 4;
@@ -61,11 +64,11 @@ __host__ __device__ inline size_t flat_fixed_bytes( int classes, int attrs, int 
 {
 	size_t b = flat_state_bytes( attrs, span ) + (size_t)classes * span * 4;
 	b = ( b + 15 ) & ~(size_t)15;
-	return b + (size_t)FLAT_ENT_CAP * 8 + (size_t)FLAT_SCRATCH * 4;
+	return b + (size_t)4 * FLAT_PC * 4 + (size_t)4 * FLAT_STEP_CAP * 8;
 }
 inline size_t flat_smem_bytes( int classes, int attrs, int tmax )
 {
-	return flat_fixed_bytes( classes, attrs, tmax ) + (size_t)FLAT_BUFS * FLAT_MIN_BUF * 16;
+	return flat_fixed_bytes( classes, attrs, tmax ) + (size_t)FLAT_ENT_CAP * 8 + (size_t)FLAT_SCRATCH * 4 + (size_t)FLAT_MIN_BUF * 16;
 }
 
 // ------------------------------------------------------------------------------------
@@ -158,18 +161,6 @@ __global__ void __launch_bounds__( 256 ) slice_fill(
 	}
 }
 
-// ------------------------------------------------------------------------------------
-// stage_window: the arrivals of the next window for every tile at once
-// ------------------------------------------------------------------------------------
-// Runs before window_flat. All CTAs compute the window's (step, source tile) prefix; then
-// each takes chunks of `chunk` arrivals, reads every arrival's record row rec[src][*]
-// (contiguous, coalesced) into shared memory and writes it out transposed, one run of
-// `chunk` consecutive entries per tile: wtab[tile][g] = rec[src_g][tile]. A window_flat
-// CTA then loads its table as one contiguous run instead of one scattered record load per
-// arrival. wsteps[k] = first entry of step k (k <= L), wsteps[MAX_WINDOW + 1] = 1 if the
-// window fits ecap (else window_flat stages by itself).
-inline size_t stage_window_smem( int ntiles, int chunk ) { return (size_t)FLAT_SCRATCH * 4 + (size_t)chunk * ( ntiles * 8 + 4 ); }
-
 // per-(step, source tile) spike counts of steps [ks, ks + ksteps) of the window starting
 // at t0 (none before `delay`) into cnts[(k - ks) * ntiles + tile], eight loads in flight
 // per thread; ends with a barrier
@@ -200,90 +191,6 @@ __device__ __forceinline__ void load_counts( net_params const & p, unsigned * cn
 	__syncthreads();
 }
 
-__global__ void __launch_bounds__( 256 ) stage_window( net_params p, int L, int chunk )
-{
-	extern __shared__ __align__( 16 ) unsigned char smem[];
-	__shared__ int scratch[33];
-	unsigned * pref = reinterpret_cast<unsigned *>( smem );                 // [FLAT_SCRATCH]
-	uint2 * srec = reinterpret_cast<uint2 *>( pref + FLAT_SCRATCH );        // [chunk][ntiles]
-	int * ssrc = reinterpret_cast<int *>( srec + (size_t)chunk * p.ntiles ); // [chunk]
-	int const tid = threadIdx.x, nt = blockDim.x, nti = p.ntiles;
-	int const M = L * nti;
-	if( M + 1 > FLAT_SCRATCH )
-	{
-		if( blockIdx.x == 0 && tid == 0 ) p.wsteps[MAX_WINDOW + 1] = 0;
-		return;
-	}
-	long long const t0 = __ldcg( &p.clock->step );
-	load_counts( p, pref, t0, 0, L, scratch );
-	int total;
-	{
-		int const per = ( M + nt - 1 ) / nt;
-		int const q0 = min( M, tid * per ), q1 = min( M, q0 + per );
-		int run = 0;
-		for( int q = q0; q < q1; q++ ) run += (int)pref[q];
-		int base = block_exclusive_scan( run, scratch, &total );
-		for( int q = q0; q < q1; q++ )
-		{
-			int const c = (int)pref[q];
-			pref[q] = (unsigned)base;
-			base += c;
-		}
-		if( tid == 0 ) pref[M] = (unsigned)total;
-	}
-	__syncthreads();
-	bool const fits = total <= p.ecap;
-	if( blockIdx.x == 0 )
-	{
-		for( int k = tid; k <= L; k += nt ) p.wsteps[k] = (int)pref[k * nti];
-		if( tid == 0 ) p.wsteps[MAX_WINDOW + 1] = fits ? 1 : 0;
-	}
-	if( !fits ) return;
-	for( int g0 = blockIdx.x * chunk; g0 < total; g0 += gridDim.x * chunk )
-	{
-		int const m = min( chunk, total - g0 );
-		if( tid < m )
-		{
-			int const g = g0 + tid;
-			int q = 0, hi = M; // last pair q with pref[q] <= g
-			while( hi - q > 1 )
-			{
-				int const mid = ( q + hi ) >> 1;
-				if( (int)pref[mid] <= g )
-					q = mid;
-				else
-					hi = mid;
-			}
-			int const k = q / nti, i = q % nti;
-			long long const t = t0 + k;
-			ssrc[tid] = __ldcg( p.ring_ids + (long long)( ( t - p.delay ) % p.ring ) * p.n + __ldg( p.tile_first + i ) + ( g - (int)pref[q] ) );
-		}
-		__syncthreads();
-		constexpr int B = 8;
-		int const items = m * nti;
-		for( int x0 = tid; x0 < items; x0 += B * nt )
-		{
-			uint2 v[B];
-#pragma unroll
-			for( int b = 0; b < B; b++ )
-			{
-				int const x = x0 + b * nt;
-				if( x < items ) v[b] = __ldg( p.slice_rec + (long long)ssrc[x / nti] * nti + x % nti );
-			}
-#pragma unroll
-			for( int b = 0; b < B; b++ )
-				if( x0 + b * nt < items ) srec[x0 + b * nt] = v[b];
-		}
-		__syncthreads();
-		for( int x = tid; x < nti * chunk; x += nt )
-		{
-			int const j = x / chunk, e = x % chunk;
-			if( e < m ) p.wtab[(long long)j * p.ecap + g0 + e] = srec[e * nti + j];
-		}
-		__syncthreads();
-	}
-}
-
 // ------------------------------------------------------------------------------------
 // window kernel
 // ------------------------------------------------------------------------------------
@@ -305,42 +212,17 @@ __device__ __forceinline__ int stage_arrivals(
 __device__ __forceinline__ int stage_offsets(
     int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int & mode );
 
-// Stage the arrivals of the steps [ks, L) of the window starting at t0, as many whole
-// steps as fit FLAT_ENT_CAP, and set the segment's mode. Returns the segment's end ke.
+// Stage the arrivals of the steps [ks, L) of the window starting at t0 (the synchronous
+// path), as many whole steps as fit FLAT_ENT_CAP, and set the segment's mode. Returns the
+// segment's end ke.
 // step_begin[k - ks] = first entry of step k and step_vec[k - ks] = first vector of step
 // k counted from the segment start, for k in [ks, ke].
 __device__ __forceinline__ int stage_table(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int * step_vec,
     int * scratch, int bufv, int & mode )
 {
-	constexpr int B = 8; // loads in flight per thread
-	int const tid = threadIdx.x, nt = blockDim.x;
-	int ke = ks, nent = 0;
-	if( p.ecap > 0 && __ldcg( p.wsteps + MAX_WINDOW + 1 ) )
-	{
-		// staged by stage_window: whole steps that fit the table, one contiguous run
-		for( int k = ks + tid; k <= L; k += nt ) step_vec[k - ks] = __ldcg( p.wsteps + k ); // scratch use
-		__syncthreads();
-		int const base = step_vec[0];
-		while( ke < L && step_vec[ke + 1 - ks] - base <= FLAT_ENT_CAP ) ke++;
-		nent = step_vec[ke - ks] - base;
-		__syncthreads();
-		for( int k = tid; k <= ke - ks; k += nt ) step_begin[k] = step_vec[k] - base;
-		uint2 const * src = p.wtab + (long long)tile * p.ecap + base;
-		for( int g0 = tid; g0 < nent; g0 += B * nt )
-		{
-			uint2 v[B];
-#pragma unroll
-			for( int b = 0; b < B; b++ )
-				if( g0 + b * nt < nent ) v[b] = __ldcg( src + g0 + b * nt );
-#pragma unroll
-			for( int b = 0; b < B; b++ )
-				if( g0 + b * nt < nent ) table[g0 + b * nt] = make_int2( (int)v[b].x, (int)v[b].y );
-		}
-		__syncthreads();
-	}
-	else
-		ke = stage_arrivals( p, cnts, table, tile, t0, ks, L, step_begin, nent, scratch );
+	int nent = 0;
+	int const ke = stage_arrivals( p, cnts, table, tile, t0, ks, L, step_begin, nent, scratch );
 	if( ke == ks )
 	{
 		mode = SEG_DIRECT; // step ks alone exceeds the table
@@ -349,8 +231,8 @@ __device__ __forceinline__ int stage_table(
 	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, bufv, mode );
 }
 
-// Per-CTA staging (when stage_window did not run or the window did not fit): the
-// (step, source tile) prefix, then every arrival's spike id and slice record. Returns ke.
+// Per-CTA staging of whole steps: the (step, source tile) prefix, then every arrival's
+// spike id and slice record. Returns ke.
 __device__ __forceinline__ int stage_arrivals(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int & nent_out, int * scratch )
 {
@@ -516,6 +398,16 @@ __device__ __forceinline__ void cp_async16( void * dst, void const * src )
 	unsigned const d = (unsigned)__cvta_generic_to_shared( dst );
 	asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"( d ), "l"( src ) : "memory" );
 }
+__device__ __forceinline__ void cp_async8( void * dst, void const * src )
+{
+	unsigned const d = (unsigned)__cvta_generic_to_shared( dst );
+	asm volatile( "cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"( d ), "l"( src ) : "memory" );
+}
+__device__ __forceinline__ void cp_async4( void * dst, void const * src )
+{
+	unsigned const d = (unsigned)__cvta_generic_to_shared( dst );
+	asm volatile( "cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"( d ), "l"( src ) : "memory" );
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wait_group 0;\n" ::: "memory" ); }
 __device__ __forceinline__ void cp_async_wait_but_one() { asm volatile( "cp.async.wait_group 1;\n" ::: "memory" ); }
@@ -562,6 +454,8 @@ __device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned
 
 // barrier of the first `threads` threads (whole warps) of the CTA
 __device__ __forceinline__ void bar_sync_first( int threads ) { asm volatile( "bar.sync 1, %0;\n" ::"r"( threads ) : "memory" ); }
+// barrier of the producer warps (the last FLAT_PRODUCERS warps)
+__device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * FLAT_PRODUCERS ) : "memory" ); }
 
 // ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
 // per round, a warp scan of their counts gives every word's offset
@@ -648,6 +542,7 @@ struct smem_state
 	}
 };
 
+
 template <typename Model>
 __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
 {
@@ -663,9 +558,12 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	__shared__ float s_c, s_sum;
 	__shared__ int step_begin[MAX_WINDOW + 1];
 	__shared__ int step_vec[MAX_WINDOW + 1];
+	// per-step staging results, slot s & 7: arrivals, vectors, ring offset, too large
+	__shared__ int m_e[8], m_v[8], m_off[8], m_big[8];
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
 	int const nwc = nw - FLAT_PRODUCERS, ncons = nwc * 32; // consumer warps first, then producers
+	int const pt = tid - ncons, npt = nt - ncons;          // producer numbering
 	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
@@ -675,10 +573,10 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	unsigned * bits2 = reinterpret_cast<unsigned *>( state + (size_t)N::size * span * 4 ); // [2][words]
 	unsigned * cnt = bits2 + 2 * words;                                                    // [C][span], inputs only
 	size_t const fixed = flat_fixed_bytes( C, (int)N::size, span );
-	int2 * table = reinterpret_cast<int2 *>( smem + fixed - (size_t)FLAT_ENT_CAP * 8 - (size_t)FLAT_SCRATCH * 4 );
-	unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
-	int const bufv = inputs ? (int)( ( (size_t)smem_bytes - fixed ) / ( 16 * FLAT_BUFS ) ) : 0;
-	uint4 * const buf0 = reinterpret_cast<uint4 *>( smem + fixed ); // FLAT_BUFS buffers of bufv vectors
+	int * pcnt = reinterpret_cast<int *>( smem + fixed - (size_t)4 * FLAT_PC * 4 - (size_t)4 * FLAT_STEP_CAP * 8 ); // [4][FLAT_PC]
+	int2 * ent = reinterpret_cast<int2 *>( pcnt + 4 * FLAT_PC );                           // [4][FLAT_STEP_CAP]
+	uint4 * const ring = reinterpret_cast<uint4 *>( smem + fixed );
+	int const rb = inputs ? (int)( ( (size_t)smem_bytes - fixed ) / 16 ) : 0; // ring vectors
 
 	window_clock_begin( p, L, dt, s_dt, &s_t0, &s_c, &s_sum );
 	long long const t0 = s_t0;
@@ -726,6 +624,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	};
 	auto compact = [&]( int k ) { compact_step( p, bits2 + ( k & 1 ) * words, words, d0, tile, t0 + k, lane ); };
 
+	int ks = L; // first step of the synchronous path
 	if( !inputs )
 	{
 		// no arrivals: every warp updates, the last warp compacts the step before while the
@@ -740,61 +639,202 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	}
 	else
 	{
-		int ks = 0;
+		// ---------------------------------------------------------------- pipelined steps
+		// producer work during step k (k < 0: the window's prologue): every stage's loads go
+		// out as asynchronous copies at once, one wait, then the scans that lay out the next
+		// stages
+		auto produce = [&]( int k ) {
+			// slices of step k + 1: entry g's vectors to ring[(off + offset(g) + j) mod rb]
+			int const sa = k + 1;
+			if( sa >= 0 && sa < L && !m_big[sa & 7] )
+			{
+				int2 const * e1 = ent + ( sa & 3 ) * FLAT_STEP_CAP;
+				int const ea = m_e[sa & 7], oa = m_off[sa & 7];
+				int const q = pt & 3, groups = npt >> 2;
+				for( int g = pt >> 2; g < ea; g += groups )
+				{
+					int2 const e = e1[g];
+					int const nv = ent_vec( e );
+					uint4 const * src = p.slices + (unsigned)e.x;
+					int o = oa + ent_off( e ) + q;
+					if( o >= rb ) o -= rb;
+					for( int j = q; j < nv; j += 4 )
+					{
+						cp_async16( ring + o, src + j );
+						o += 4;
+						if( o >= rb ) o -= rb;
+					}
+				}
+			}
+			// slice records of step k + 2's arrivals, over their spike ids
+			int const sb = k + 2;
+			bool const do_b = sb >= 0 && sb < L && !m_big[sb & 7];
+			if( do_b )
+			{
+				int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
+				int const eb = m_e[sb & 7];
+				for( int g = pt; g < eb; g += npt ) cp_async8( e2 + g, p.slice_rec + (long long)e2[g].x * p.ntiles + tile );
+			}
+			// spike ids of step k + 3 (its per-source-tile counts are scanned)
+			int const sc = k + 3;
+			if( sc >= 0 && sc < L && !m_big[sc & 7] )
+			{
+				int const * pc = pcnt + ( sc & 3 ) * FLAT_PC;
+				int2 * e3 = ent + ( sc & 3 ) * FLAT_STEP_CAP;
+				int const ec = m_e[sc & 7];
+				long long const slot = ( ( t0 + sc - p.delay ) % p.ring ) * (long long)p.n;
+				for( int g = pt; g < ec; g += npt )
+				{
+					int lo = 0, hi = p.ntiles; // last source tile i with pc[i] <= g
+					while( hi - lo > 1 )
+					{
+						int const mid = ( lo + hi ) >> 1;
+						if( pc[mid] <= g )
+							lo = mid;
+						else
+							hi = mid;
+					}
+					cp_async4( &e3[g].x, p.ring_ids + slot + __ldg( p.tile_first + lo ) + ( g - pc[lo] ) );
+				}
+			}
+			// per-source-tile spike counts of step k + 4 (none before `delay`)
+			int const sd = k + 4;
+			bool const do_d = sd >= 0 && sd < L;
+			if( do_d )
+			{
+				int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
+				long long const t = t0 + sd;
+				for( int i = pt; i < p.ntiles; i += npt )
+				{
+					if( t >= p.delay )
+						cp_async4( pc + i, p.ring_cnt + ( ( t - p.delay ) % p.ring ) * p.ntiles + i );
+					else
+						pc[i] = 0;
+				}
+			}
+			cp_async_commit();
+			cp_async_wait_all();
+			bar_sync_producers();
+			// the two scans, one warp each, while another producer warp compacts
+			int const pw = pt >> 5;
+			if( do_b && pw == 0 )
+			{
+				// ring layout of step k + 2: per-entry vector offsets and the step's place
+				int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
+				int const eb = m_e[sb & 7];
+				int carry = 0;
+				for( int g0 = 0; g0 < eb; g0 += 32 )
+				{
+					int const g = g0 + lane;
+					int2 e = g < eb ? e2[g] : make_int2( 0, 0 );
+					int const nv = g < eb ? ent_vec( e ) : 0;
+					int const incl = warp_inclusive_scan( nv );
+					if( g < eb )
+					{
+						e.y = ent_len( e ) | ( ( carry + incl - nv ) << 12 );
+						e2[g] = e;
+					}
+					carry += __shfl_sync( 0xffffffffu, incl, 31 );
+				}
+				if( lane == 0 )
+				{
+					int const prev_v = sb > 0 ? m_v[( sb - 1 ) & 7] : 0, prev_off = sb > 0 ? m_off[( sb - 1 ) & 7] : 0;
+					m_v[sb & 7] = carry;
+					int o = prev_off + prev_v;
+					if( o >= rb ) o -= rb;
+					m_off[sb & 7] = o;
+					// two steps live in the ring at once: the one counted and the one copied
+					if( carry + prev_v > rb || carry >= ( 1 << FLAT_P_BITS ) ) m_big[sb & 7] = 1;
+				}
+			}
+			if( do_d && pw == 1 )
+			{
+				// exclusive prefix of step k + 4's per-source-tile counts: its arrivals
+				int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
+				int carry = 0;
+				for( int i0 = 0; i0 < p.ntiles; i0 += 32 )
+				{
+					int const i = i0 + lane;
+					int const c = i < p.ntiles ? pc[i] : 0;
+					int const incl = warp_inclusive_scan( c );
+					if( i < p.ntiles ) pc[i] = carry + incl - c;
+					carry += __shfl_sync( 0xffffffffu, incl, 31 );
+				}
+				if( lane == 0 )
+				{
+					pc[p.ntiles] = carry;
+					m_e[sd & 7] = carry;
+					m_big[sd & 7] = carry > FLAT_STEP_CAP ? 1 : 0;
+				}
+			}
+		};
+
+		if( p.flat_sync ) ks = 0;
+		if( warp >= nwc && ks == L )
+			for( int k = -4; k < 0; k++ )
+			{
+				produce( k );
+				bar_sync_producers();
+			}
+		__syncthreads();
+		for( int k = 0; k < ks; k++ )
+		{
+			if( m_big[k & 7] )
+			{
+				ks = k; // this step and the rest of the window take the synchronous path
+				break;
+			}
+			if( warp < nwc )
+			{
+				if( t0 + k >= p.delay )
+				{
+					// count the ring region [off, off + V) of step k
+					int const v = m_v[k & 7], o = m_off[k & 7];
+#pragma unroll 2
+					for( int x = tid; x < v; x += ncons )
+					{
+						int y = o + x;
+						if( y >= rb ) y -= rb;
+						uint4 const w = ring[y];
+						count_index( cnt, w.x & 0xFFFFu );
+						count_index( cnt, w.x >> 16 );
+						count_index( cnt, w.y & 0xFFFFu );
+						count_index( cnt, w.y >> 16 );
+						count_index( cnt, w.z & 0xFFFFu );
+						count_index( cnt, w.z >> 16 );
+						count_index( cnt, w.w & 0xFFFFu );
+						count_index( cnt, w.w >> 16 );
+					}
+				}
+				bar_sync_first( ncons ); // counts complete
+				update( k, nwc );
+			}
+			else
+			{
+				produce( k );
+				if( k > 0 && warp == nw - 1 ) compact( k - 1 );
+			}
+			__syncthreads(); // step k updated, step k + 1's slices in the ring
+		}
+		int const last = ks - 1; // the last pipelined step, not compacted yet
+		if( last >= 0 && warp == nw - 1 ) compact( last );
+		__syncthreads();
+	}
+
+	// ---------------------------------------------------------------- synchronous path
+	// window-wide staging from step ks on, its table, scratch and buffer in the slice ring
+	if( ks < L )
+	{
+		int2 * table = reinterpret_cast<int2 *>( ring );
+		unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
+		uint4 * buf = reinterpret_cast<uint4 *>( cnts + FLAT_SCRATCH );
+		int const bufv = rb - ( FLAT_ENT_CAP * 8 + FLAT_SCRATCH * 4 ) / 16;
 		while( ks < L )
 		{
 			int mode;
 			int const ke = stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch, bufv, mode );
-			if( mode == SEG_PIPE )
+			for( int k = ks; k < ke; k++ )
 			{
-				// producers copy step k + 2 while consumers count and update step k
-				int const pt = tid - ncons, npt = nt - ncons;
-				auto issue_step = [&]( int k ) {
-					issue_piece( p, table, step_begin[k - ks], step_begin[k + 1 - ks], buf0 + ( k % FLAT_BUFS ) * bufv, pt, npt );
-					cp_async_commit();
-				};
-				if( warp >= nwc )
-				{
-					issue_step( ks );
-					if( ks + 1 < ke )
-					{
-						issue_step( ks + 1 );
-						cp_async_wait_but_one();
-					}
-					else
-						cp_async_wait_all();
-				}
-				__syncthreads();
-				for( int k = ks; k < ke; k++ )
-				{
-					if( warp < nwc )
-					{
-						if( t0 + k >= p.delay )
-							count_buffer( buf0 + ( k % FLAT_BUFS ) * bufv, step_vec[k + 1 - ks] - step_vec[k - ks], cnt, tid, ncons );
-						bar_sync_first( ncons ); // counts complete
-						update( k, nwc );
-					}
-					else
-					{
-						// the buffer of step k + 2 was last read by step k - 1's counting
-						if( k + 2 < ke )
-						{
-							issue_step( k + 2 );
-							cp_async_wait_but_one(); // step k + 1's copies are complete
-						}
-						else
-							cp_async_wait_all();
-						if( k > ks && warp == nw - 1 ) compact( k - 1 );
-					}
-					__syncthreads(); // step k updated, step k + 1's slices in place
-				}
-				if( warp == nw - 1 ) compact( ke - 1 );
-				__syncthreads();
-			}
-			else
-			{
-				// step ks alone, every warp
-				int const k = ks;
 				long long const t = t0 + k;
 				if( t >= p.delay )
 				{
@@ -802,25 +842,25 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 					{
 						// the direct path of window_counts, its scratch in the (unused) table
 						int * pref = reinterpret_cast<int *>( table );
-						int4 * sb = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( table ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
+						int4 * sbuf = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( table ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
 						net_params q = p;
 						q.tile = span; // counter rows are span long
-						deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sb, scratch );
+						deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sbuf, scratch );
 					}
 					else
 					{
-						// pieces that fit all the slice buffers together
-						int const e = step_begin[1];
-						int const sv = step_vec[1] - step_vec[0];
-						for( int a = 0, b = 0; b < e; )
+						// slices in pieces that fit the buffer
+						int const e = step_begin[k + 1 - ks];
+						int const sv = step_vec[k + 1 - ks] - step_vec[k - ks];
+						for( int a = step_begin[k - ks], b = a; b < e; )
 						{
 							a = b;
-							b = piece_end( table, a, e, FLAT_BUFS * bufv );
-							issue_piece( p, table, a, b, buf0, tid, nt );
+							b = piece_end( table, a, e, bufv );
+							issue_piece( p, table, a, b, buf, tid, nt );
 							cp_async_commit();
 							cp_async_wait_all();
 							__syncthreads();
-							count_buffer( buf0, piece_vectors( table, a, b, e, sv ), cnt, tid, nt );
+							count_buffer( buf, piece_vectors( table, a, b, e, sv ), cnt, tid, nt );
 							__syncthreads();
 						}
 					}

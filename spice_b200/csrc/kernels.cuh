@@ -65,9 +65,7 @@ struct net_params
 	uint4 const * slices;    // tile-major 16-bit slices (window_flat)
 	uint2 const * slice_rec; // [n][ntiles] { first vector, length } (window_flat)
 	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
-	uint2 * wtab;            // [ntiles][ecap] the window's arrivals per tile (stage_window)
-	int * wsteps;            // [MAX_WINDOW + 2] first arrival of every step, validity flag
-	int ecap;                // arrivals per window wtab holds (0: no stage_window)
+	int flat_sync;           // window_flat: every step on the synchronous path
 };
 
 template <typename T>

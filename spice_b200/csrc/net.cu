@@ -234,9 +234,7 @@ struct spk_net
 	int flat_smem = 0;   // dynamic shared memory of a window_flat launch
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
-	dbuf wtab, wsteps;      // per-window arrival tables of stage_window
-	int ecap = 0;           // arrivals per window stage_window handles (0: off)
-	int stage_chunk = 0;    // arrivals a stage_window CTA transposes at once
+	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
 
 	~spk_net()
 	{
@@ -267,9 +265,7 @@ struct spk_net
 		p.slices = slices.as<uint4 const>();
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
-		p.wtab = wtab.as<uint2>();
-		p.wsteps = wsteps.as<int>();
-		p.ecap = ecap;
+		p.flat_sync = flat_sync;
 		return p;
 	}
 
@@ -277,7 +273,7 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + wtab.bytes + wsteps.bytes;
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -365,14 +361,7 @@ struct spk_net
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
 		}
 		else if( flat )
-		{
-			if( ecap > 0 )
-			{
-				spk::stage_window<<<2 * sms, 256, spk::stage_window_smem( tc.ntiles, stage_chunk ), stream>>>( p, L, stage_chunk );
-				CK( cudaGetLastError() );
-			}
 			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
-		}
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
 		CK( cudaGetLastError() );
@@ -658,7 +647,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 			char const * tiling = getenv( "SPK_TILES" );
 			std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
 			                                                                       : balanced_tiles( segs, n, dev_sms, tmax, tmax_free );
-			if( (int)first.size() - 1 < spk::FLAT_SCRATCH )
+			if( (int)first.size() < spk::FLAT_PC )
 			{
 				// the largest tile with inputs sets the shared-memory floor (tiles without
 				// inputs need less than it per neuron)
@@ -737,22 +726,10 @@ void build_slices( spk_net & net )
 	require( all < ( 1ULL << 32 ), "graph too large for 32-bit slice records" );
 	std::vector<int> inputs( nt );
 	for( int j = 0; j < nt; j++ ) inputs[j] = tot[j] > 0;
+	char const * sync = getenv( "SPK_FLAT_SYNC" );
+	net.flat_sync = sync && !strcmp( sync, "1" );
 	net.tile_inputs.alloc( (size_t)nt * 4 );
 	CK( cudaMemcpyAsync( net.tile_inputs.p, inputs.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
-	// stage_window: window tables for up to FLAT_STAGE_CAP arrivals (SPK_STAGE=cta: off)
-	char const * stage = getenv( "SPK_STAGE" );
-	net.ecap = 0;
-	if( nt <= 1024 && (long long)net.max_window() * nt + 1 <= spk::FLAT_SCRATCH && !( stage && !strcmp( stage, "cta" ) ) )
-	{
-		net.stage_chunk = (int)std::min<long long>( 32, ( 49152 - 1024 - (long long)spk::FLAT_SCRATCH * 4 ) / ( nt * 8LL + 4 ) );
-		if( net.stage_chunk >= 1 )
-		{
-			net.ecap = spk::FLAT_STAGE_CAP;
-			net.wtab.alloc( (size_t)nt * net.ecap * sizeof( uint2 ) );
-			net.wsteps.alloc( ( spk::MAX_WINDOW + 2 ) * sizeof( int ) );
-			CK( cudaMemsetAsync( net.wsteps.p, 0, net.wsteps.bytes, net.stream ) );
-		}
-	}
 	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ) );
 	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)nt * 8, cudaMemcpyHostToDevice, net.stream ) );
 	switch( net.model )

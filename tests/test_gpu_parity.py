@@ -243,20 +243,20 @@ def test_errors():
 
 # ----------------------------------------------------------------------- window kernel paths
 @pytest.mark.parametrize("n,delay,steps,stage,deg", [
-    (60_000, 15, 60, None, 16),      # ~300 arrivals per step: one table per window from stage_window
-    (150_000, 15, 60, None, 16),     # ~750 per step: stage_window's table read in two segments
-    (400_000, 15, 60, None, 16),     # ~2000 per step: more than stage_window holds, per-CTA staging
-    (150_000, 15, 60, "cta", 16),    # per-CTA staging throughout
-    (1_700_000, 4, 24, None, 16),    # > 8192 arrivals in one step: the direct path inside window_flat
-    (1_000_000, 4, 16, None, 800),   # ~5000 slices per tile and step: more than a buffer, in pieces
-    (400_000, 8, 32, "uniform", 800),  # equal 1 k-neuron tiles
+    (60_000, 15, 60, None, 16),       # ~300 arrivals per step: the step pipeline
+    (150_000, 15, 60, None, 16),      # ~750 per step: the step pipeline
+    (400_000, 15, 60, None, 16),      # ~2000 per step: more than a step table, synchronous path
+    (150_000, 15, 60, "sync", 16),    # synchronous path throughout
+    (1_700_000, 4, 24, None, 16),     # > 6144 arrivals in one step: the direct path inside window_flat
+    (1_000_000, 4, 16, None, 800),    # ~5000 slices per tile and step: more than a buffer, in pieces
+    (400_000, 8, 32, "uniform", 800), # equal 1 k-neuron tiles
 ])
 def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage, deg):
     """window_flat (staged table, balanced tiles, slice buffers) against window_counts,
     itself checked against the oracle above, on nets too large for the oracle to step
     quickly."""
     layout = Layout(n, deg / n)
-    env = {"cta": ("SPK_STAGE", "cta"), "uniform": ("SPK_TILES", "uniform")}
+    env = {"sync": ("SPK_FLAT_SYNC", "1"), "uniform": ("SPK_TILES", "uniform")}
     for f in (stage.split("+") if stage else []):
         os.environ[env[f][0]] = env[f][1]
     try:
