@@ -130,7 +130,7 @@ def measured_peaks():
 
 def profile_traffic():
     """DRAM bytes per launch of the window kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "window_counts_brunel_1e9.json")
+    path = os.path.join(ROOT, "profiles", "window_flat_brunel_1e9.json")
     try:
         with open(path) as f:
             return float(json.load(f)["dram_bytes_per_launch_full_size"])
@@ -254,12 +254,16 @@ def run_ours(args, rank, world):
 
     bio = args.steps * S * DT
     value = (ms_max / 1e3) / (bio * world)
-    # roofline of the window kernel (the only kernel of the timed region)
-    mean_degree = sum(p * (d1 - d0) for (s, d, p), (d0, d1) in zip(CONNS, [(POPS[0], POPS[0] + POPS[1])] * 2))
+    # roofline of the window kernel (the only kernel of the timed region), algorithmic bytes
+    # per step as the path defines them: every arriving synapse's 4-byte index, one 4-byte
+    # pivot per (spike, tile), the neuron state read and written by propagation and by the
+    # update, and the spike ids
     n = sum(POPS)
+    mean_degree = sum(POPS[a] * p * POPS[b] for a, b, p in CONNS) / n
     state_bytes = 8  # V, Twait
-    bytes_per_step = spikes_per_step * mean_degree * 4 + spikes_per_step * info.num_tiles * 8
-    bytes_per_window = DELAY * bytes_per_step + 2 * n * state_bytes
+    bytes_per_step = (spikes_per_step * mean_degree * 4 + spikes_per_step * info.num_tiles * 4 + 4 * n * state_bytes
+                      + spikes_per_step * 4)
+    bytes_per_window = DELAY * bytes_per_step
     launches = args.steps * windows_per_step
     t_launch = (ms / 1e3) / launches
     peak, peak_kind = measured_peaks()
@@ -275,7 +279,7 @@ def run_ours(args, rank, world):
                            "tiles": info.num_tiles, "tile_size": info.tile_size, "setup_s": setup_s,
                            "spikes_per_step": spikes_per_step},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": traffic, "peak_kind": peak_kind, "kernel": "window_counts<brunel>",
+                             "traffic": traffic, "peak_kind": peak_kind, "kernel": "window_flat<brunel>",
                              "bytes_per_launch": bytes_per_window, "launch_us": t_launch * 1e6},
                 "e2e": {"value": e2e_wall / (S * DT * world), "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": int(statistics.median(d2h))},

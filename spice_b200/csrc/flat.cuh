@@ -40,7 +40,10 @@
 namespace spk
 {
 constexpr int FLAT_THREADS = 1024;    // threads of a window_flat CTA (one CTA per SM)
-constexpr int FLAT_PRODUCERS = 8;     // warps that stage, copy slices and compact spikes
+#ifndef SPK_FLAT_PRODUCERS
+#define SPK_FLAT_PRODUCERS 12
+#endif
+constexpr int FLAT_PRODUCERS = SPK_FLAT_PRODUCERS; // warps that stage, copy slices and compact spikes
 constexpr int FLAT_PC = 1032;         // per-source-tile counts of one step (ntiles + 1 <= FLAT_PC)
 constexpr int FLAT_STEP_CAP = 1024;   // arrivals of one step the pipeline stages
 constexpr int FLAT_ENT_CAP = 6144;    // arrivals per segment of the synchronous path
@@ -643,7 +646,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 		// producer work during step k (k < 0: the window's prologue): every stage's loads go
 		// out as asynchronous copies at once, one wait, then the scans that lay out the next
 		// stages
-		auto produce = [&]( int k ) {
+		auto produce = [&]( int k, int pt, int npt, bool all ) {
 			// slices of step k + 1: entry g's vectors to ring[(off + offset(g) + j) mod rb]
 			int const sa = k + 1;
 			if( sa >= 0 && sa < L && !m_big[sa & 7] )
@@ -714,7 +717,10 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 			}
 			cp_async_commit();
 			cp_async_wait_all();
-			bar_sync_producers();
+			if( all )
+				__syncthreads();
+			else
+				bar_sync_producers();
 			// the two scans, one warp each, while another producer warp compacts
 			int const pw = pt >> 5;
 			if( do_b && pw == 0 )
@@ -770,11 +776,12 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 		};
 
 		if( p.flat_sync ) ks = 0;
-		if( warp >= nwc && ks == L )
+		if( ks == L )
 			for( int k = -4; k < 0; k++ )
 			{
-				produce( k );
-				bar_sync_producers();
+				// the prologue: every warp stages (nobody counts yet)
+				produce( k, tid, nt, true );
+				__syncthreads();
 			}
 		__syncthreads();
 		for( int k = 0; k < ks; k++ )
@@ -811,7 +818,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 			}
 			else
 			{
-				produce( k );
+				produce( k, pt, npt, false );
 				if( k > 0 && warp == nw - 1 ) compact( k - 1 );
 			}
 			__syncthreads(); // step k updated, step k + 1's slices in the ring
