@@ -184,7 +184,11 @@ __device__ __forceinline__ void load_counts( net_params const & p, unsigned * cn
 			{
 				int const k = ks + q / p.ntiles, i = q % p.ntiles;
 				long long const t = t0 + k;
-				if( t >= p.delay ) v[b] = __ldcg( p.ring_cnt + (long long)( ( t - p.delay ) % p.ring ) * p.ntiles + i );
+				if( t >= p.delay )
+				{
+					wait_published( p, i, t - p.delay );
+					v[b] = __ldcg( p.ring_cnt + (long long)( ( t - p.delay ) % p.ring ) * p.ntiles + i );
+				}
 			}
 		}
 #pragma unroll
@@ -461,7 +465,8 @@ __device__ __forceinline__ void bar_sync_first( int threads ) { asm volatile( "b
 __device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * FLAT_PRODUCERS ) : "memory" ); }
 
 // ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
-// per round, a warp scan of their counts gives every word's offset
+// per round, a warp scan of their counts gives every word's offset; then the step is
+// published to the other tiles
 __device__ __forceinline__ void compact_step( net_params const & p, unsigned const * bits, int words, int d0, int tile, long long t, int lane )
 {
 	int const slot_out = (int)( t % p.ring );
@@ -483,6 +488,10 @@ __device__ __forceinline__ void compact_step( net_params const & p, unsigned con
 		done += __shfl_sync( 0xffffffffu, incl, 31 );
 	}
 	if( lane == 0 ) p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
+	// every lane's ring writes, then the flag that publishes them
+	__threadfence();
+	__syncwarp();
+	if( lane == 0 ) publish_step( p, tile, t );
 }
 
 // neuron state of the tile: shared memory [attrs][span] <-> registers / global memory
@@ -546,6 +555,11 @@ struct smem_state
 };
 
 
+// Launches of up to `delay` steps read only spikes of earlier launches. A longer launch
+// (a cooperative launch: every CTA resident) reads spikes other tiles publish during it:
+// before staging a step, a tile waits until every source tile has published the step
+// `delay` earlier. With the pipeline checking five steps ahead that is a step before its
+// own current one (delay >= 6), so the slowest tile never waits and every wait ends.
 template <typename Model>
 __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
 {
@@ -553,10 +567,11 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	using Tup = typename N::template apply<reg_tuple>;
 	constexpr int C = N::input_classes;
 	static_assert( C >= 1, "window_flat needs a model with input classes" );
+	constexpr int DT_AHEAD = MAX_WINDOW / 2; // compensated dt computed this many steps ahead
 
 	extern __shared__ __align__( 128 ) unsigned char smem[];
 	__shared__ int scratch[33];
-	__shared__ float s_dt[MAX_WINDOW];
+	__shared__ float s_dt[MAX_WINDOW]; // dt of step k at k % MAX_WINDOW
 	__shared__ long long s_t0;
 	__shared__ float s_c, s_sum;
 	__shared__ int step_begin[MAX_WINDOW + 1];
@@ -566,7 +581,6 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
 	int const nwc = nw - FLAT_PRODUCERS, ncons = nwc * 32; // consumer warps first, then producers
-	int const pt = tid - ncons, npt = nt - ncons;          // producer numbering
 	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
@@ -581,8 +595,34 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	uint4 * const ring = reinterpret_cast<uint4 *>( smem + fixed );
 	int const rb = inputs ? (int)( ( (size_t)smem_bytes - fixed ) / 16 ) : 0; // ring vectors
 
-	window_clock_begin( p, L, dt, s_dt, &s_t0, &s_c, &s_sum );
+	// the simulated clock: thread 0 advances the Kahan-compensated dt DT_AHEAD steps ahead
+	if( tid == 0 )
+	{
+		clock_state const cs = *p.clock;
+		float c = cs.c, sum = cs.sum;
+		for( int k = 0; k < min( L, DT_AHEAD ); k++ )
+		{
+			s_dt[k % MAX_WINDOW] = kahan_add( c, sum, dt );
+			if( blockIdx.x == 0 ) p.dt_ring[( cs.step + k ) % DT_RING] = s_dt[k % MAX_WINDOW];
+		}
+		s_t0 = cs.step;
+		s_c = c;
+		s_sum = sum;
+	}
+	__syncthreads();
 	long long const t0 = s_t0;
+	auto advance_clock = [&]( int k ) { // at step k, by thread 0: the dt of step k + DT_AHEAD
+		int const ka = k + DT_AHEAD;
+		if( tid == 0 && ka < L )
+		{
+			float c = s_c, sum = s_sum;
+			float const d = kahan_add( c, sum, dt );
+			s_dt[ka % MAX_WINDOW] = d;
+			s_c = c;
+			s_sum = sum;
+			if( blockIdx.x == 0 ) p.dt_ring[( t0 + ka ) % DT_RING] = d;
+		}
+	};
 	smem_state<N>::from_global( p.attr, d0, span, state );
 	// counters start at zero; the update zeroes every counter it consumes
 	if( inputs )
@@ -595,6 +635,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 		long long const t = t0 + k;
 		bool const arrivals = inputs && t >= p.delay;
 		unsigned * bits = bits2 + ( k & 1 ) * words;
+		float const dtk = s_dt[k % MAX_WINDOW];
 		for( int base = warp * 32; base < span; base += nws * 32 )
 		{
 			int const local = base + lane;
@@ -618,7 +659,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 						}
 					}
 				device_backend bak( p.seed, i, (uint32_t)t );
-				fired = N::update( it, s_dt[k], info, bak );
+				fired = N::update( it, dtk, info, bak );
 				smem_state<N>::store( st, state, span, local );
 			}
 			unsigned const word = __ballot_sync( 0xffffffffu, fired );
@@ -627,222 +668,246 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 	};
 	auto compact = [&]( int k ) { compact_step( p, bits2 + ( k & 1 ) * words, words, d0, tile, t0 + k, lane ); };
 
-	int ks = L; // first step of the synchronous path
 	if( !inputs )
 	{
 		// no arrivals: every warp updates, the last warp compacts the step before while the
 		// others update the next one (its bits are in the other half)
 		for( int k = 0; k < L; k++ )
 		{
+			advance_clock( k );
 			update( k, nw );
 			__syncthreads();
-			if( warp == nw - 1 ) compact( k );
+			if( warp == nw - 1 )
+			{
+				// the ring slot of step t held step t - 2 delay: wait until every tile has
+				// published step t - delay, so none still stages from the overwritten step
+				// (tiles with inputs are bounded by their own waits)
+				for( int i = lane; i < p.ntiles; i += 32 ) wait_published( p, i, t0 + k - p.delay );
+				__syncwarp();
+				compact( k );
+			}
 		}
 		__syncthreads();
 	}
 	else
 	{
-		// ---------------------------------------------------------------- pipelined steps
-		// producer work during step k (k < 0: the window's prologue): every stage's loads go
-		// out as asynchronous copies at once, one wait, then the scans that lay out the next
-		// stages
-		auto produce = [&]( int k, int pt, int npt, bool all ) {
-			// slices of step k + 1: entry g's vectors to ring[(off + offset(g) + j) mod rb]
-			int const sa = k + 1;
-			if( sa >= 0 && sa < L && !m_big[sa & 7] )
-			{
-				int2 const * e1 = ent + ( sa & 3 ) * FLAT_STEP_CAP;
-				int const ea = m_e[sa & 7], oa = m_off[sa & 7];
-				int const q = pt & 3, groups = npt >> 2;
-				for( int g = pt >> 2; g < ea; g += groups )
+		int k = 0; // next step to simulate
+		while( k < L )
+		{
+			// ------------------------------------------------------------ pipelined steps
+			int const kb = k; // the pipeline (re)starts at step kb
+			// producer work during step j (j < kb: the prologue): every stage's loads go out
+			// as asynchronous copies at once, one wait, then the scans that lay out the
+			// next stages
+			auto produce = [&]( int j, int pt, int npt, bool all ) {
+				// slices of step j + 1: entry g's vectors to ring[(off + offset(g) + v) mod rb]
+				int const sa = j + 1;
+				if( sa >= kb && sa < L && !m_big[sa & 7] )
 				{
-					int2 const e = e1[g];
-					int const nv = ent_vec( e );
-					uint4 const * src = p.slices + (unsigned)e.x;
-					int o = oa + ent_off( e ) + q;
-					if( o >= rb ) o -= rb;
-					for( int j = q; j < nv; j += 4 )
+					int2 const * e1 = ent + ( sa & 3 ) * FLAT_STEP_CAP;
+					int const ea = m_e[sa & 7], oa = m_off[sa & 7];
+					int const q = pt & 3, groups = npt >> 2;
+					for( int g = pt >> 2; g < ea; g += groups )
 					{
-						cp_async16( ring + o, src + j );
-						o += 4;
+						int2 const e = e1[g];
+						int const nv = ent_vec( e );
+						uint4 const * src = p.slices + (unsigned)e.x;
+						int o = oa + ent_off( e ) + q;
 						if( o >= rb ) o -= rb;
+						for( int v = q; v < nv; v += 4 )
+						{
+							cp_async16( ring + o, src + v );
+							o += 4;
+							if( o >= rb ) o -= rb;
+						}
 					}
 				}
-			}
-			// slice records of step k + 2's arrivals, over their spike ids
-			int const sb = k + 2;
-			bool const do_b = sb >= 0 && sb < L && !m_big[sb & 7];
-			if( do_b )
-			{
-				int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
-				int const eb = m_e[sb & 7];
-				for( int g = pt; g < eb; g += npt ) cp_async8( e2 + g, p.slice_rec + (long long)e2[g].x * p.ntiles + tile );
-			}
-			// spike ids of step k + 3 (its per-source-tile counts are scanned)
-			int const sc = k + 3;
-			if( sc >= 0 && sc < L && !m_big[sc & 7] )
-			{
-				int const * pc = pcnt + ( sc & 3 ) * FLAT_PC;
-				int2 * e3 = ent + ( sc & 3 ) * FLAT_STEP_CAP;
-				int const ec = m_e[sc & 7];
-				long long const slot = ( ( t0 + sc - p.delay ) % p.ring ) * (long long)p.n;
-				for( int g = pt; g < ec; g += npt )
+				// slice records of step j + 2's arrivals, over their spike ids
+				int const sb = j + 2;
+				bool const do_b = sb >= kb && sb < L && !m_big[sb & 7];
+				if( do_b )
 				{
-					int lo = 0, hi = p.ntiles; // last source tile i with pc[i] <= g
-					while( hi - lo > 1 )
+					int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
+					int const eb = m_e[sb & 7];
+					for( int g = pt; g < eb; g += npt ) cp_async8( e2 + g, p.slice_rec + (long long)e2[g].x * p.ntiles + tile );
+				}
+				// spike ids of step j + 3 (its per-source-tile counts are scanned)
+				int const sc = j + 3;
+				if( sc >= kb && sc < L && !m_big[sc & 7] )
+				{
+					int const * pc = pcnt + ( sc & 3 ) * FLAT_PC;
+					int2 * e3 = ent + ( sc & 3 ) * FLAT_STEP_CAP;
+					int const ec = m_e[sc & 7];
+					long long const slot = ( ( t0 + sc - p.delay ) % p.ring ) * (long long)p.n;
+					for( int g = pt; g < ec; g += npt )
 					{
-						int const mid = ( lo + hi ) >> 1;
-						if( pc[mid] <= g )
-							lo = mid;
+						int lo = 0, hi = p.ntiles; // last source tile i with pc[i] <= g
+						while( hi - lo > 1 )
+						{
+							int const mid = ( lo + hi ) >> 1;
+							if( pc[mid] <= g )
+								lo = mid;
+							else
+								hi = mid;
+						}
+						cp_async4( &e3[g].x, p.ring_ids + slot + __ldg( p.tile_first + lo ) + ( g - pc[lo] ) );
+					}
+				}
+				// per-source-tile spike counts of step j + 4 (none before `delay`): every
+				// source tile has published the step they fired in (checked during the step
+				// before, or here in the prologue)
+				int const sd = j + 4;
+				bool const do_d = sd >= kb && sd < L;
+				if( do_d )
+				{
+					int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
+					long long const t = t0 + sd;
+					for( int i = pt; i < p.ntiles; i += npt )
+					{
+						if( t >= p.delay )
+						{
+							if( j < kb ) wait_published( p, i, t - p.delay );
+							cp_async4( pc + i, p.ring_cnt + ( ( t - p.delay ) % p.ring ) * p.ntiles + i );
+						}
 						else
-							hi = mid;
+							pc[i] = 0;
 					}
-					cp_async4( &e3[g].x, p.ring_ids + slot + __ldg( p.tile_first + lo ) + ( g - pc[lo] ) );
 				}
-			}
-			// per-source-tile spike counts of step k + 4 (none before `delay`)
-			int const sd = k + 4;
-			bool const do_d = sd >= 0 && sd < L;
-			if( do_d )
-			{
-				int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
-				long long const t = t0 + sd;
-				for( int i = pt; i < p.ntiles; i += npt )
+				// publication of the spikes step j + 5 reads, checked while the copies above
+				// are in flight (a step before its own one for delay >= 6: no wait in practice)
+				if( j + 5 >= kb && j + 5 < L && j + 5 + t0 >= p.delay )
+					for( int i = pt; i < p.ntiles; i += npt ) wait_published( p, i, t0 + j + 5 - p.delay );
+				cp_async_commit();
+				cp_async_wait_all();
+				if( all )
+					__syncthreads();
+				else
+					bar_sync_producers();
+				// the two scans, one warp each, while another producer warp compacts
+				int const pw = pt >> 5;
+				if( do_b && pw == 0 )
 				{
-					if( t >= p.delay )
-						cp_async4( pc + i, p.ring_cnt + ( ( t - p.delay ) % p.ring ) * p.ntiles + i );
-					else
-						pc[i] = 0;
-				}
-			}
-			cp_async_commit();
-			cp_async_wait_all();
-			if( all )
-				__syncthreads();
-			else
-				bar_sync_producers();
-			// the two scans, one warp each, while another producer warp compacts
-			int const pw = pt >> 5;
-			if( do_b && pw == 0 )
-			{
-				// ring layout of step k + 2: per-entry vector offsets and the step's place
-				int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
-				int const eb = m_e[sb & 7];
-				int carry = 0;
-				for( int g0 = 0; g0 < eb; g0 += 32 )
-				{
-					int const g = g0 + lane;
-					int2 e = g < eb ? e2[g] : make_int2( 0, 0 );
-					int const nv = g < eb ? ent_vec( e ) : 0;
-					int const incl = warp_inclusive_scan( nv );
-					if( g < eb )
+					// ring layout of step j + 2: per-entry vector offsets and the step's place
+					int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
+					int const eb = m_e[sb & 7];
+					int carry = 0;
+					for( int g0 = 0; g0 < eb; g0 += 32 )
 					{
-						e.y = ent_len( e ) | ( ( carry + incl - nv ) << 12 );
-						e2[g] = e;
+						int const g = g0 + lane;
+						int2 e = g < eb ? e2[g] : make_int2( 0, 0 );
+						int const nv = g < eb ? ent_vec( e ) : 0;
+						int const incl = warp_inclusive_scan( nv );
+						if( g < eb )
+						{
+							e.y = ent_len( e ) | ( ( carry + incl - nv ) << 12 );
+							e2[g] = e;
+						}
+						carry += __shfl_sync( 0xffffffffu, incl, 31 );
 					}
-					carry += __shfl_sync( 0xffffffffu, incl, 31 );
+					if( lane == 0 )
+					{
+						int const prev_v = sb > kb ? m_v[( sb - 1 ) & 7] : 0, prev_off = sb > kb ? m_off[( sb - 1 ) & 7] : 0;
+						m_v[sb & 7] = carry;
+						int o = prev_off + prev_v;
+						if( o >= rb ) o -= rb;
+						m_off[sb & 7] = o;
+						// two steps live in the ring at once: the one counted and the one copied
+						if( carry + prev_v > rb || carry >= ( 1 << FLAT_P_BITS ) ) m_big[sb & 7] = 1;
+					}
 				}
-				if( lane == 0 )
+				if( do_d && pw == 1 )
 				{
-					int const prev_v = sb > 0 ? m_v[( sb - 1 ) & 7] : 0, prev_off = sb > 0 ? m_off[( sb - 1 ) & 7] : 0;
-					m_v[sb & 7] = carry;
-					int o = prev_off + prev_v;
-					if( o >= rb ) o -= rb;
-					m_off[sb & 7] = o;
-					// two steps live in the ring at once: the one counted and the one copied
-					if( carry + prev_v > rb || carry >= ( 1 << FLAT_P_BITS ) ) m_big[sb & 7] = 1;
+					// exclusive prefix of step j + 4's per-source-tile counts: its arrivals
+					int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
+					int carry = 0;
+					for( int i0 = 0; i0 < p.ntiles; i0 += 32 )
+					{
+						int const i = i0 + lane;
+						int const c = i < p.ntiles ? pc[i] : 0;
+						int const incl = warp_inclusive_scan( c );
+						if( i < p.ntiles ) pc[i] = carry + incl - c;
+						carry += __shfl_sync( 0xffffffffu, incl, 31 );
+					}
+					if( lane == 0 )
+					{
+						pc[p.ntiles] = carry;
+						m_e[sd & 7] = carry;
+						m_big[sd & 7] = carry > FLAT_STEP_CAP ? 1 : 0;
+					}
 				}
-			}
-			if( do_d && pw == 1 )
-			{
-				// exclusive prefix of step k + 4's per-source-tile counts: its arrivals
-				int * pc = pcnt + ( sd & 3 ) * FLAT_PC;
-				int carry = 0;
-				for( int i0 = 0; i0 < p.ntiles; i0 += 32 )
-				{
-					int const i = i0 + lane;
-					int const c = i < p.ntiles ? pc[i] : 0;
-					int const incl = warp_inclusive_scan( c );
-					if( i < p.ntiles ) pc[i] = carry + incl - c;
-					carry += __shfl_sync( 0xffffffffu, incl, 31 );
-				}
-				if( lane == 0 )
-				{
-					pc[p.ntiles] = carry;
-					m_e[sd & 7] = carry;
-					m_big[sd & 7] = carry > FLAT_STEP_CAP ? 1 : 0;
-				}
-			}
-		};
+			};
 
-		if( p.flat_sync ) ks = 0;
-		if( ks == L )
-			for( int k = -4; k < 0; k++ )
+			int ks = L; // first step of a synchronous stretch, if any
+			if( !p.flat_sync )
 			{
-				// the prologue: every warp stages (nobody counts yet)
-				produce( k, tid, nt, true );
-				__syncthreads();
-			}
-		__syncthreads();
-		for( int k = 0; k < ks; k++ )
-		{
-			if( m_big[k & 7] )
-			{
-				ks = k; // this step and the rest of the window take the synchronous path
-				break;
-			}
-			if( warp < nwc )
-			{
-				if( t0 + k >= p.delay )
+				for( int j = kb - 4; j < kb; j++ )
 				{
-					// count the ring region [off, off + V) of step k
-					int const v = m_v[k & 7], o = m_off[k & 7];
+					// the prologue: every warp stages (nobody counts yet)
+					produce( j, tid, nt, true );
+					__syncthreads();
+				}
+				for( ; k < L; k++ )
+				{
+					if( m_big[k & 7] )
+					{
+						ks = k; // this step takes the synchronous path
+						break;
+					}
+					advance_clock( k );
+					if( warp < nwc )
+					{
+						if( t0 + k >= p.delay )
+						{
+							// count the ring region [off, off + V) of step k
+							int const v = m_v[k & 7], o = m_off[k & 7];
 #pragma unroll 2
-					for( int x = tid; x < v; x += ncons )
-					{
-						int y = o + x;
-						if( y >= rb ) y -= rb;
-						uint4 const w = ring[y];
-						count_index( cnt, w.x & 0xFFFFu );
-						count_index( cnt, w.x >> 16 );
-						count_index( cnt, w.y & 0xFFFFu );
-						count_index( cnt, w.y >> 16 );
-						count_index( cnt, w.z & 0xFFFFu );
-						count_index( cnt, w.z >> 16 );
-						count_index( cnt, w.w & 0xFFFFu );
-						count_index( cnt, w.w >> 16 );
+							for( int x = tid; x < v; x += ncons )
+							{
+								int y = o + x;
+								if( y >= rb ) y -= rb;
+								uint4 const w = ring[y];
+								count_index( cnt, w.x & 0xFFFFu );
+								count_index( cnt, w.x >> 16 );
+								count_index( cnt, w.y & 0xFFFFu );
+								count_index( cnt, w.y >> 16 );
+								count_index( cnt, w.z & 0xFFFFu );
+								count_index( cnt, w.z >> 16 );
+								count_index( cnt, w.w & 0xFFFFu );
+								count_index( cnt, w.w >> 16 );
+							}
+						}
+						bar_sync_first( ncons ); // counts complete
+						update( k, nwc );
 					}
+					else
+					{
+						// step k - 1 is published before any stage of step k waits for it
+						if( k > kb && warp == nw - 1 ) compact( k - 1 );
+						produce( k, tid - ncons, nt - ncons, false );
+					}
+					__syncthreads(); // step k updated, step k + 1's slices in the ring
 				}
-				bar_sync_first( ncons ); // counts complete
-				update( k, nwc );
+				if( k > kb && warp == nw - 1 ) compact( k - 1 ); // the last pipelined step
+				__syncthreads();
 			}
 			else
-			{
-				produce( k, pt, npt, false );
-				if( k > 0 && warp == nw - 1 ) compact( k - 1 );
-			}
-			__syncthreads(); // step k updated, step k + 1's slices in the ring
-		}
-		int const last = ks - 1; // the last pipelined step, not compacted yet
-		if( last >= 0 && warp == nw - 1 ) compact( last );
-		__syncthreads();
-	}
+				ks = k;
+			if( ks >= L ) break;
 
-	// ---------------------------------------------------------------- synchronous path
-	// window-wide staging from step ks on, its table, scratch and buffer in the slice ring
-	if( ks < L )
-	{
-		int2 * table = reinterpret_cast<int2 *>( ring );
-		unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
-		uint4 * buf = reinterpret_cast<uint4 *>( cnts + FLAT_SCRATCH );
-		int const bufv = rb - ( FLAT_ENT_CAP * 8 + FLAT_SCRATCH * 4 ) / 16;
-		while( ks < L )
-		{
+			// ------------------------------------------------------------ synchronous steps
+			// staging of whole steps (those whose spikes are published already: fewer than
+			// `delay` steps ahead), table, scratch and buffer in the slice ring; back to the
+			// pipeline after the first segment unless every step goes this way
+			int2 * table = reinterpret_cast<int2 *>( ring );
+			unsigned * cnts = reinterpret_cast<unsigned *>( table + FLAT_ENT_CAP );
+			uint4 * buf = reinterpret_cast<uint4 *>( cnts + FLAT_SCRATCH );
+			int const bufv = rb - ( FLAT_ENT_CAP * 8 + FLAT_SCRATCH * 4 ) / 16;
 			int mode;
-			int const ke = stage_table( p, cnts, table, tile, t0, ks, L, step_begin, step_vec, scratch, bufv, mode );
-			for( int k = ks; k < ke; k++ )
+			int const ke = stage_table( p, cnts, table, tile, t0, ks, min( L, ks + p.delay ), step_begin, step_vec, scratch, bufv, mode );
+			for( int kk = ks; kk < ke; kk++ )
 			{
-				long long const t = t0 + k;
+				advance_clock( kk );
+				long long const t = t0 + kk;
 				if( t >= p.delay )
 				{
 					if( mode == SEG_DIRECT )
@@ -852,14 +917,16 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 						int4 * sbuf = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( table ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
 						net_params q = p;
 						q.tile = span; // counter rows are span long
+						for( int i = tid; i < p.ntiles; i += nt ) wait_published( p, i, t - p.delay );
+						__syncthreads();
 						deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sbuf, scratch );
 					}
 					else
 					{
 						// slices in pieces that fit the buffer
-						int const e = step_begin[k + 1 - ks];
-						int const sv = step_vec[k + 1 - ks] - step_vec[k - ks];
-						for( int a = step_begin[k - ks], b = a; b < e; )
+						int const e = step_begin[kk + 1 - ks];
+						int const sv = step_vec[kk + 1 - ks] - step_vec[kk - ks];
+						for( int a = step_begin[kk - ks], b = a; b < e; )
 						{
 							a = b;
 							b = piece_end( table, a, e, bufv );
@@ -873,12 +940,12 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 					}
 				}
 				__syncthreads();
-				update( k, nw );
+				update( kk, nw );
 				__syncthreads();
-				if( warp == nw - 1 ) compact( k );
+				if( warp == nw - 1 ) compact( kk );
 				__syncthreads();
 			}
-			ks = ke;
+			k = ke;
 		}
 	}
 

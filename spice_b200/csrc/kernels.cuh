@@ -40,8 +40,10 @@ constexpr int DT_RING = 128;    // per-step dt history (>= MAX_WINDOW)
 enum error_bits
 {
 	ERR_BAD_TARGET = 1, // an edge pointed outside its tile slice (corrupt pivots/graph)
-	ERR_OVERFLOW = 2
+	ERR_OVERFLOW = 2,
+	ERR_TIMEOUT = 4     // a wait for another tile's spikes gave up (window_flat)
 };
+constexpr int WAIT_LIMIT = 1 << 20; // polls of a bounded wait (about a second)
 
 struct conn_dev
 {
@@ -66,6 +68,7 @@ struct net_params
 	uint2 const * slice_rec; // [n][ntiles] { first vector, length } (window_flat)
 	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
 	int flat_sync;           // window_flat: every step on the synchronous path
+	long long * done_step;   // [ntiles] last step whose spikes the tile has published
 };
 
 template <typename T>
@@ -156,6 +159,34 @@ __device__ __forceinline__ void window_clock_begin( net_params const & p, int L,
 			for( int k = 0; k < L; k++ ) p.dt_ring[( cs.step + k ) % DT_RING] = s_dt[k];
 	}
 	__syncthreads();
+}
+
+// Publication of a tile's spikes (window_flat): after the ring entries of step t are
+// written, every writer fences and the tile's flag is released; a reader acquires the flag
+// before it reads the ring. A wait polls with a limit, then flags ERR_TIMEOUT and returns.
+__device__ __forceinline__ void publish_step( net_params const & p, int tile, long long t )
+{
+	asm volatile( "st.release.gpu.global.s64 [%0], %1;" ::"l"( p.done_step + tile ), "l"( t ) : "memory" );
+}
+__device__ __forceinline__ long long published( net_params const & p, int i )
+{
+	long long v;
+	asm volatile( "ld.acquire.gpu.global.s64 %0, [%1];" : "=l"( v ) : "l"( p.done_step + i ) : "memory" );
+	return v;
+}
+__device__ __forceinline__ void wait_published( net_params const & p, int i, long long t )
+{
+	if( t < 0 ) return;
+	for( int it = 0; published( p, i ) < t; it++ )
+	{
+		// after one wait has given up, every other wait of the launch returns at once
+		if( it >= WAIT_LIMIT || ( *(int volatile *)p.err & ERR_TIMEOUT ) )
+		{
+			atomicOr( p.err, ERR_TIMEOUT );
+			return;
+		}
+		__nanosleep( 256 );
+	}
 }
 
 __device__ __forceinline__ void window_clock_end( net_params const & p, int L, long long t0, float c, float sum )

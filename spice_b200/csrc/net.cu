@@ -235,6 +235,8 @@ struct spk_net
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
 	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
+	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
+	bool persistent = false; // run() as one cooperative window_flat launch (delay >= 6)
 
 	~spk_net()
 	{
@@ -266,6 +268,7 @@ struct spk_net
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
 		p.flat_sync = flat_sync;
+		p.done_step = done_step.as<long long>();
 		return p;
 	}
 
@@ -273,7 +276,7 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes;
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + done_step.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -332,6 +335,13 @@ struct spk_net
 				flat_smem = optin - (int)fa.sharedSizeBytes;
 				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
 				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				// one launch for a whole run: every tile's CTA resident at once (cooperative
+				// launch), and the step pipeline never waits on a step not yet simulated
+				int coop = 0, per_sm = 0;
+				CK( cudaDeviceGetAttribute( &coop, cudaDevAttrCooperativeLaunch, device ) );
+				CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_flat<Model>, tc.threads, flat_smem ) );
+				char const * pers = getenv( "SPK_PERSIST" );
+				persistent = coop && delay >= 6 && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
 				return;
 			}
 		with_window_kernel<Model>( [&]( auto kernel ) {
@@ -442,9 +452,46 @@ struct spk_net
 		graph_len = len;
 	}
 
+	// all of a run's steps as cooperative launches of window_flat (section on persistence in
+	// flat.cuh)
+	template <typename Model>
+	void launch_persistent_model( int L )
+	{
+		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
+		{
+			auto p = params();
+			int smem = flat_smem;
+			float d = dt;
+			void * args[] = { &p, &L, &d, &smem };
+			CK( cudaLaunchCooperativeKernel( (void const *)spk::window_flat<Model>, dim3( tc.ntiles ), dim3( tc.threads ), args, (size_t)smem, stream ) );
+		}
+	}
+	void launch_persistent( int L )
+	{
+		switch( model )
+		{
+		case SPK_VOGELS_ABBOTT: launch_persistent_model<spice::vogels_abbott>( L ); break;
+		case SPK_BRUNEL: launch_persistent_model<spice::brunel>( L ); break;
+		case SPK_SYNTH: launch_persistent_model<spice::synth>( L ); break;
+		default: break;
+		}
+	}
+
 	void run( unsigned long long nsteps )
 	{
 		flush();
+		if( persistent )
+		{
+			while( nsteps > 0 )
+			{
+				int const L = (int)std::min<unsigned long long>( nsteps, 1u << 30 );
+				steps += L;
+				launch_persistent( L );
+				launched += L;
+				nsteps -= L;
+			}
+			return;
+		}
 		int const len = max_window();
 		unsigned long long const windows = std::min<unsigned long long>( nsteps / len, 512 );
 		if( windows >= 2 )
@@ -728,6 +775,8 @@ void build_slices( spk_net & net )
 	for( int j = 0; j < nt; j++ ) inputs[j] = tot[j] > 0;
 	char const * sync = getenv( "SPK_FLAT_SYNC" );
 	net.flat_sync = sync && !strcmp( sync, "1" );
+	net.done_step.alloc( (size_t)nt * sizeof( long long ) );
+	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
 	net.tile_inputs.alloc( (size_t)nt * 4 );
 	CK( cudaMemcpyAsync( net.tile_inputs.p, inputs.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
 	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ) );

@@ -274,3 +274,28 @@ def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage, deg):
     assert ca.max() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
     for x, y in zip(a.neurons(), b.neurons()):
         assert np.array_equal(x, y)
+
+
+# ----------------------------------------------------------------- one launch per run()
+@pytest.mark.parametrize("model,pops,conns,delay,steps", [
+    ("brunel", [10_000, 10_000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 600),  # Poisson tiles run ahead, bounded
+    ("synth", [300_000], [(0, 0, 16 / 300_000)], 6, 200),               # delay 6: checks the step before
+    ("synth", [400_000], [(0, 0, 16 / 400_000)], 8, 120),               # > 1024 arrivals a step: pipeline restarts
+    ("vogels_abbott", [4000], [(0, 0, 0.02)], 8, 500),
+])
+def test_persistent_run_matches_windows(model, pops, conns, delay, steps):
+    """run() as one cooperative launch in which tiles wait for each other's published
+    spikes, against the same steps as windowed launches (checked against the oracle above)."""
+    layout = Layout(pops, conns)
+    a = Snn(model, layout, delay=delay, seed=5, graph_seed=11)
+    os.environ["SPK_PERSIST"] = "0"
+    try:
+        b = Snn(model, layout, delay=delay, seed=5, graph_seed=11)
+    finally:
+        del os.environ["SPK_PERSIST"]
+    a.run(steps)
+    b.run(steps)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+    for i in range(2 * delay):  # the spike ring the long launch left behind
+        assert np.array_equal(a.step(out=True), b.step(out=True)), i
