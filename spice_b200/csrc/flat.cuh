@@ -17,8 +17,9 @@
 //   - load the slice records of step k + 2's arrivals and lay out their ring offsets,
 //   - load the spike ids of step k + 3 (the per-source-tile spike counts, scanned),
 //   - load the per-source-tile spike counts of step k + 4,
-//   - and compact the fired neurons of step k - 1 in ascending order into the spike ring,
-// each stage one global-memory round trip that a whole step hides. The consumers count
+// each stage one global-memory round trip that a whole step hides, while the last warp
+// compacts the fired neurons of step k - 1 in ascending order into the spike ring and
+// publishes them. The consumers count
 // step k from the ring, one 16-byte vector per thread at a time with a shared-memory
 // atomic per index; a consumer-only barrier; then they replay the counts through the
 // model's receive(), update every neuron and zero the counters they consumed. The tile's
@@ -461,8 +462,9 @@ __device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned
 
 // barrier of the first `threads` threads (whole warps) of the CTA
 __device__ __forceinline__ void bar_sync_first( int threads ) { asm volatile( "bar.sync 1, %0;\n" ::"r"( threads ) : "memory" ); }
-// barrier of the producer warps (the last FLAT_PRODUCERS warps)
-__device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * FLAT_PRODUCERS ) : "memory" ); }
+// barrier of the producer warps (FLAT_PRODUCERS - 1 warps before the last one, which
+// compacts and publishes)
+__device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * ( FLAT_PRODUCERS - 1 ) ) : "memory" ); }
 
 // ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
 // per round, a warp scan of their counts gives every word's offset; then the step is
@@ -682,8 +684,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 				// the ring slot of step t held step t - 2 delay: wait until every tile has
 				// published step t - delay, so none still stages from the overwritten step
 				// (tiles with inputs are bounded by their own waits)
-				for( int i = lane; i < p.ntiles; i += 32 ) wait_published( p, i, t0 + k - p.delay );
-				__syncwarp();
+				warp_wait_all_published( p, t0 + k - p.delay );
 				compact( k );
 			}
 		}
@@ -702,7 +703,8 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 			auto produce = [&]( int j, int pt, int npt, bool all ) {
 				// slices of step j + 1: entry g's vectors to ring[(off + offset(g) + v) mod rb]
 				int const sa = j + 1;
-				if( sa >= kb && sa < L && !m_big[sa & 7] )
+				bool const do_a = sa >= kb && sa < L && !m_big[sa & 7];
+				if( do_a )
 				{
 					int2 const * e1 = ent + ( sa & 3 ) * FLAT_STEP_CAP;
 					int const ea = m_e[sa & 7], oa = m_off[sa & 7];
@@ -791,17 +793,29 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 					int2 * e2 = ent + ( sb & 3 ) * FLAT_STEP_CAP;
 					int const eb = m_e[sb & 7];
 					int carry = 0;
-					for( int g0 = 0; g0 < eb; g0 += 32 )
+					// four entries per lane and round (two 16-byte loads)
+					for( int g0 = 0; g0 < eb; g0 += 128 )
 					{
-						int const g = g0 + lane;
-						int2 e = g < eb ? e2[g] : make_int2( 0, 0 );
-						int const nv = g < eb ? ent_vec( e ) : 0;
-						int const incl = warp_inclusive_scan( nv );
-						if( g < eb )
+						int const g = g0 + 4 * lane;
+						int4 const a01 = g < eb ? reinterpret_cast<int4 const *>( e2 )[g >> 1] : make_int4( 0, 0, 0, 0 );
+						int4 const a23 = g + 2 < eb ? reinterpret_cast<int4 const *>( e2 )[( g >> 1 ) + 1] : make_int4( 0, 0, 0, 0 );
+						int2 e[4] = { make_int2( a01.x, a01.y ), make_int2( a01.z, a01.w ), make_int2( a23.x, a23.y ), make_int2( a23.z, a23.w ) };
+						int nv[4], sum = 0;
+#pragma unroll
+						for( int u = 0; u < 4; u++ )
 						{
-							e.y = ent_len( e ) | ( ( carry + incl - nv ) << 12 );
-							e2[g] = e;
+							nv[u] = g + u < eb ? ent_vec( e[u] ) : 0;
+							sum += nv[u];
 						}
+						int const incl = warp_inclusive_scan( sum );
+						int off = carry + incl - sum;
+#pragma unroll
+						for( int u = 0; u < 4; u++ )
+							if( g + u < eb )
+							{
+								e2[g + u] = make_int2( e[u].x, ent_len( e[u] ) | ( off << 12 ) );
+								off += nv[u];
+							}
 						carry += __shfl_sync( 0xffffffffu, incl, 31 );
 					}
 					if( lane == 0 )
@@ -879,12 +893,14 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 						bar_sync_first( ncons ); // counts complete
 						update( k, nwc );
 					}
-					else
+					else if( warp == nw - 1 )
 					{
-						// step k - 1 is published before any stage of step k waits for it
-						if( k > kb && warp == nw - 1 ) compact( k - 1 );
-						produce( k, tid - ncons, nt - ncons, false );
+						// the publisher warp: step k - 1's spikes to the ring, fenced, then its
+						// flag (the fence waits for the stores; no producer waits on it)
+						if( k > kb ) compact( k - 1 );
 					}
+					else
+						produce( k, tid - ncons, nt - ncons - 32, false );
 					__syncthreads(); // step k updated, step k + 1's slices in the ring
 				}
 				if( k > kb && warp == nw - 1 ) compact( k - 1 ); // the last pipelined step

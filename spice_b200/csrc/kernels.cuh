@@ -189,6 +189,25 @@ __device__ __forceinline__ void wait_published( net_params const & p, int i, lon
 	}
 }
 
+// every tile has published step t: lanes of a warp read the flags of tiles lane, lane + 32,
+// ... at once (relaxed), one acquire fence when all are there, else the bounded wait
+__device__ __forceinline__ void warp_wait_all_published( net_params const & p, long long t )
+{
+	if( t < 0 ) return;
+	bool ok = true;
+	for( int i = threadIdx.x & 31; i < p.ntiles; i += 32 )
+	{
+		long long v;
+		asm volatile( "ld.relaxed.gpu.global.s64 %0, [%1];" : "=l"( v ) : "l"( p.done_step + i ) : "memory" );
+		ok = ok && v >= t;
+	}
+	if( __all_sync( 0xffffffffu, ok ) )
+		asm volatile( "fence.acq_rel.gpu;" ::: "memory" );
+	else
+		for( int i = threadIdx.x & 31; i < p.ntiles; i += 32 ) wait_published( p, i, t );
+	__syncwarp();
+}
+
 __device__ __forceinline__ void window_clock_end( net_params const & p, int L, long long t0, float c, float sum )
 {
 	__syncthreads();
