@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--syn", type=float, default=1e9,
                     help="total synapses of the Brunel net (the benchmark is 1e9; smaller sizes serve profiling)")
+    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched"],
+                    help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop")
+    ap.add_argument("--nets", type=int, default=256, help="batched: number of nets")
+    ap.add_argument("--bio", type=float, default=1.0, help="batched: biological seconds per net")
     args = ap.parse_args()
     if args.syn != 1e9:
         # samples/main.cpp:1283,1395: N = sqrt(syn / 0.05), two populations of N / 2
@@ -294,12 +298,120 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+BATCH_MODELS = ("vogels_abbott", "brunel", "brunel_with_plasticity")
+
+
+def batched_specs(count, seed=0):
+    """Nets drawn uniformly from {VA, Brunel, Brunel+} with synapse counts log-uniform in
+    1e5-5e7; N = sqrt(syn / p_eff) with p_eff 0.02 (VA layout{N, 0.02}) and 0.05 (Brunel's
+    two populations of N/2 at p = 0.1 into the second), delay 8 (VA, the published runs)
+    and 15 (Brunel, Brunel+); seeds 1..count."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        model = BATCH_MODELS[int(rng.integers(0, 3))]
+        syn = float(np.exp(rng.uniform(np.log(1e5), np.log(5e7))))
+        if model == "vogels_abbott":
+            n = max(64, int((syn / 0.02) ** 0.5))
+            pops, conns, delay = [n], [(0, 0, 0.02)], 8
+        else:
+            half = max(32, int((syn / 0.05) ** 0.5) // 2)
+            pops, conns, delay = [half, half], [(0, 1, 0.1), (1, 1, 0.1)], 15
+        specs.append({"model": model, "pops": pops, "conns": conns, "delay": delay, "seed": i + 1, "syn": syn})
+    return specs
+
+
+def tile_targets(specs, sms):
+    """Tiles per net of a batch: each net's share of the SMs by its expected work
+    (synapses plus a per-neuron update cost), at least one."""
+    work = [s["syn"] * 0.01 + 1000.0 * sum(s["pops"]) for s in specs]
+    total = sum(work)
+    return [max(1, int(round(sms * w / total))) for w in work]
+
+
+def run_batched(args, rank, world):
+    """Batched workload: the same nets stepped (a) one at a time, the plain per-job loop
+    (spice_bench/paper_plots.cpp:184-231 steps one net after another), and (b) together in
+    one Batch. Setup is excluded from both; each arm's wall time is CUDA-event timed on the
+    device around its steps. Reports both and the ratio."""
+    import torch
+
+    from spice_b200 import Batch, Layout, Snn
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    specs = batched_specs(args.nets)
+    steps = int(round(args.bio / DT))
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+
+    def make(s):
+        return Snn(s["model"], Layout(s["pops"], s["conns"]), dt=DT, delay=s["delay"], seed=s["seed"],
+                   graph_seed=1000 + s["seed"], device=dev)
+
+    # (a) plain loop: each net alone, its own default tiling, one after another
+    t0 = time.perf_counter()
+    plain = [make(s) for s in specs]
+    for n in plain:
+        n.sync()
+    setup_plain = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    t0 = time.perf_counter()
+    for n in plain:
+        n.run(steps)
+        n.sync()
+    wall_plain = time.perf_counter() - t0
+    syn_total = sum(n.num_synapses() for n in plain)
+    for n in plain:
+        n.close()
+    del plain
+
+    # (b) batch: re-tiled by work share, one Batch
+    t0 = time.perf_counter()
+    nets = [make(s) for s in specs]
+    batch = Batch(device=dev)
+    for n, t in zip(nets, tile_targets(specs, sms)):
+        n.set_tile_target(t)
+        batch.add(n)
+    for n in nets:
+        n.sync()
+    setup_batch = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.run(steps)
+    for n in nets:
+        n.sync()
+    wall_batch = time.perf_counter() - t0
+    clk = clocks.stop()
+    tiles = sum(n.info().num_tiles for n in nets)
+    batch.close()
+    for n in nets:
+        n.close()
+
+    bio_total = len(specs) * steps * DT
+    if rank == 0:
+        counts = {m: sum(1 for s in specs if s["model"] == m) for m in BATCH_MODELS}
+        line = {"metric": "batched synapse-seconds per wall second", "value": syn_total * steps * DT / wall_batch,
+                "unit": "syn*bio_s/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": wall_batch * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"batched_{len(specs)}_nets", "nets": counts, "synapses_total": syn_total,
+                           "syn_range": [1e5, 5e7], "bio_s_per_net": steps * DT, "dt": DT, "tiles_total": tiles},
+                "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch},
+                "plain_loop": {"wall_s": wall_plain, "wall_per_bio": wall_plain / bio_total, "setup_s": setup_plain,
+                               "value": syn_total * steps * DT / wall_plain},
+                "speedup_vs_plain_loop": wall_plain / wall_batch, "clocks": clk}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "batched":
+            run_batched(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:

@@ -177,6 +177,29 @@ int spk_net_synapses( spk_net * net, void * const * attrs );
  * attribute, 'f' (float32) or 'i' (int32) in types (neuron attributes, then synapse). */
 int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs, char * types, int types_cap );
 
+/* ---- batching: many independent nets stepped together ------------------------------
+ * The reference steps one net per snn object (spice/cuda/snn.d.cpp:224-289); a workload
+ * of many small nets is a host loop over them (spice_bench/paper_plots.cpp:184-231). A
+ * batch advances all its nets by the same number of steps with shared kernel launches:
+ * each launch runs every tile of every net of one model for up to that net's delay in
+ * steps, one CTA per (net, tile). Results are identical to stepping each net alone. */
+typedef struct spk_batch spk_batch;
+
+/* Re-tile a net, before its first step, into about `target` tiles (>= 1): a net sharing
+ * the GPU with others in a batch takes fewer CTAs than a net alone (one per SM). */
+int spk_net_set_tile_target( spk_net * net, int target );
+
+int spk_batch_create( spk_batch ** out, int device );
+/* Nets of the models without plasticity (SPK_VOGELS_ABBOTT, SPK_BRUNEL, SPK_SYNTH), on the
+ * batch's device; a net belongs to at most one batch. */
+int spk_batch_add( spk_batch * batch, spk_net * net );
+int spk_batch_remove( spk_batch * batch, spk_net * net );
+/* Advance every net of the batch by `nsteps` steps (asynchronous against the host up to
+ * the launches; each net's own stream is ordered after them, so spk_net_sync and the
+ * state exports of a net see the batch's steps). */
+int spk_batch_run( spk_batch * batch, uint64_t nsteps );
+int spk_batch_destroy( spk_batch * batch );
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,12 @@ def library():
         "spk_net_neurons": (I, [VP, P(VP)]),
         "spk_net_synapses": (I, [VP, P(VP)]),
         "spk_model_attrs": (I, [I, P(I), P(I), C.c_char_p, I]),
+        "spk_net_set_tile_target": (I, [VP, I]),
+        "spk_batch_create": (I, [P(VP), I]),
+        "spk_batch_add": (I, [VP, VP]),
+        "spk_batch_remove": (I, [VP, VP]),
+        "spk_batch_run": (I, [VP, U64]),
+        "spk_batch_destroy": (I, [VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -314,3 +320,58 @@ class Snn:
     def set_synapses(self, arrays):
         arrs = [np.ascontiguousarray(a, dtype=t) for a, t in zip(arrays, self._sdt)]
         _check(library().spk_net_set_synapses(self._h, _arr_ptrs(arrs)))
+
+    def set_tile_target(self, target):
+        """Re-tile (before the first step) into about `target` tiles, for sharing the GPU."""
+        _check(library().spk_net_set_tile_target(self._h, int(target)))
+
+
+class Batch:
+    """Many independent nets stepped together by shared launches (one CTA per net tile).
+
+    Nets of the models without plasticity; each keeps its own state, stream and results,
+    identical to stepping it alone. A net is in at most one batch.
+    """
+
+    def __init__(self, device=0):
+        self._h = C.c_void_p()
+        self._nets = []
+        _check(library().spk_batch_create(C.byref(self._h), int(device)))
+
+    def add(self, net):
+        _check(library().spk_batch_add(self._h, net._h))
+        self._nets.append(net)
+
+    def remove(self, net):
+        _check(library().spk_batch_remove(self._h, net._h))
+        self._nets.remove(net)
+
+    @property
+    def nets(self):
+        return list(self._nets)
+
+    def run(self, nsteps):
+        """Advance every net by nsteps steps."""
+        _check(library().spk_batch_run(self._h, int(nsteps)))
+
+    def sync(self):
+        for n in self._nets:
+            n.sync()
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(library().spk_batch_destroy(self._h))
+            self._h = C.c_void_p()
+            self._nets = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -563,7 +563,7 @@ struct smem_state
 // `delay` earlier. With the pipeline checking five steps ahead that is a step before its
 // own current one (delay >= 6), so the slowest tile never waits and every wait ends.
 template <typename Model>
-__global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
+__device__ __forceinline__ void window_flat_body( net_params const & p, int const tile, int L, float dt, int smem_bytes )
 {
 	using N = typename Model::neuron;
 	using Tup = typename N::template apply<reg_tuple>;
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
 	int const nwc = nw - FLAT_PRODUCERS, ncons = nwc * 32; // consumer warps first, then producers
-	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
+	int const d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
 	snn_info const info{ p.n };
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 		for( int k = 0; k < min( L, DT_AHEAD ); k++ )
 		{
 			s_dt[k % MAX_WINDOW] = kahan_add( c, sum, dt );
-			if( blockIdx.x == 0 ) p.dt_ring[( cs.step + k ) % DT_RING] = s_dt[k % MAX_WINDOW];
+			if( tile == 0 ) p.dt_ring[( cs.step + k ) % DT_RING] = s_dt[k % MAX_WINDOW];
 		}
 		s_t0 = cs.step;
 		s_c = c;
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 			s_dt[ka % MAX_WINDOW] = d;
 			s_c = c;
 			s_sum = sum;
-			if( blockIdx.x == 0 ) p.dt_ring[( t0 + ka ) % DT_RING] = d;
+			if( tile == 0 ) p.dt_ring[( t0 + ka ) % DT_RING] = d;
 		}
 	};
 	smem_state<N>::from_global( p.attr, d0, span, state );
@@ -967,5 +967,25 @@ __global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, 
 
 	smem_state<N>::to_global( p.attr, d0, span, state );
 	window_clock_end( p, L, t0, s_c, s_sum );
+}
+
+// one net: CTA j runs tile j
+template <typename Model>
+__global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat( net_params p, int L, float dt, int smem_bytes )
+{
+	window_flat_body<Model>( p, blockIdx.x, L, dt, smem_bytes );
+}
+
+// Many independent nets of one model in one launch (batching): CTA b runs tile jobs[b].y
+// of net jobs[b].x for jobs[b].z steps of dt __int_as_float(jobs[b].w); every net's steps
+// read only spikes of earlier launches (jobs[b].z <= that net's delay).
+template <typename Model>
+__global__ void __launch_bounds__( FLAT_THREADS, 1 ) window_flat_batch( net_params const * nets, int4 const * jobs, int smem_bytes )
+{
+	__shared__ net_params s_p;
+	int4 const j = jobs[blockIdx.x];
+	if( threadIdx.x == 0 ) s_p = nets[j.x];
+	__syncthreads();
+	if( j.z > 0 ) window_flat_body<Model>( s_p, j.y, j.z, __int_as_float( j.w ), smem_bytes );
 }
 } // namespace spk

@@ -215,7 +215,7 @@ __device__ __forceinline__ void window_clock_end( net_params const & p, int L, l
 	{
 		__threadfence();
 		unsigned const prev = atomicAdd( &p.clock->done, 1u );
-		if( prev == gridDim.x - 1 )
+		if( prev == (unsigned)p.ntiles - 1 ) // the net's last CTA (batched launches run several nets)
 		{
 			p.clock->step = t0 + L;
 			p.clock->c = c;

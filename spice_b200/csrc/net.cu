@@ -237,6 +237,8 @@ struct spk_net
 	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
 	bool persistent = false; // run() as one cooperative window_flat launch (delay >= 6)
+	std::vector<double> seg_start, seg_cost; // expected work per neuron stretch (tiling)
+	spk_batch * batch = nullptr;             // the batch holding this net, if any
 
 	~spk_net()
 	{
@@ -335,6 +337,12 @@ struct spk_net
 				flat_smem = optin - (int)fa.sharedSizeBytes;
 				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
 				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				cudaFuncAttributes fb{};
+				CK( cudaFuncGetAttributes( &fb, spk::window_flat_batch<Model> ) );
+				require( (int)fb.sharedSizeBytes <= (int)fa.sharedSizeBytes + (int)sizeof( spk::net_params ) + 256, "batched kernel shared memory" );
+				flat_smem = std::min( flat_smem, optin - (int)fb.sharedSizeBytes );
+				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				CK( cudaFuncSetAttribute( spk::window_flat_batch<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
 				// one launch for a whole run: every tile's CTA resident at once (cooperative
 				// launch), and the step pipeline never waits on a step not yet simulated
 				int coop = 0, per_sm = 0;
@@ -659,6 +667,43 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 	CK( cudaMemcpy( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice ) );
 }
 
+// window_flat's tiling of a net into at most about `target` work-balanced tiles (target =
+// the SM count for a net alone; fewer for a net that shares the GPU in a batch). Sets
+// net.flat and the tiles; false if the net does not fit window_flat.
+bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int target )
+{
+	long long const n = net.n;
+	int optin = 0;
+	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net.device ) );
+	// largest tile whose counters, state, tables and minimal slice ring fit (with room for
+	// the kernel's static shared memory), and whose counter indices fit 16 bits
+	int tmax = spk::FLAT_MAX_TILE;
+	while( tmax >= 128 && ( spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), tmax ) + 4096 > (size_t)optin ||
+	                        (long long)net.classes() * tmax >= spk::SLICE_PAD ) )
+		tmax -= 32;
+	// tiles without inputs keep only their neuron state and fired bits
+	int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * net.neuron_attrs() + 8 ) ) / 32 * 32 );
+	if( tmax < 128 ) return false;
+	char const * tiling = getenv( "SPK_TILES" );
+	std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
+	                                                                       : balanced_tiles( segs, n, std::max( 1, target ), tmax, tmax_free );
+	if( (int)first.size() >= spk::FLAT_PC ) return false;
+	// the largest tile with inputs sets the shared-memory floor (tiles without inputs need
+	// less than it per neuron)
+	int span = 0;
+	size_t si = 0;
+	for( size_t i = 0; i + 1 < first.size(); i++ )
+	{
+		while( si + 1 < segs.size() && segs[si + 1].start <= first[i] ) si++;
+		if( segs[si].cost > UPDATE_COST || first[i + 1] - first[i] <= tmax ) span = std::max( span, first[i + 1] - first[i] );
+	}
+	net.flat = true;
+	net.flat_tmax = ( span + 31 ) / 32 * 32;
+	net.tc = { spk::FLAT_THREADS, 1, net.flat_tmax, (int)first.size() - 1 };
+	set_tiles( net, first );
+	return true;
+}
+
 // buffers + pivots; edges must be filled before build_pivots is enqueued
 void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs )
 {
@@ -675,43 +720,16 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 
 	// window kernel and tiling: window_flat with work-balanced tiles (SPK_TILES=uniform keeps
 	// equal tiles, SPK_KERNEL=direct selects window_counts)
+	net.seg_start.clear();
+	net.seg_cost.clear();
+	for( auto const & g : segs )
+	{
+		net.seg_start.push_back( (double)g.start );
+		net.seg_cost.push_back( g.cost );
+	}
 	net.flat = false;
 	char const * kern = getenv( "SPK_KERNEL" );
-	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) )
-	{
-		int optin = 0;
-		CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net.device ) );
-		// largest tile whose counters, state, table and two minimal slice buffers fit (with
-		// room for the kernel's static shared memory), and whose counter indices fit 16 bits
-		int tmax = spk::FLAT_MAX_TILE;
-		while( tmax >= 128 && ( spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), tmax ) + 4096 > (size_t)optin ||
-		                        (long long)net.classes() * tmax >= spk::SLICE_PAD ) )
-			tmax -= 32;
-		// tiles without inputs keep only their neuron state and fired bits
-		int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * net.neuron_attrs() + 8 ) ) / 32 * 32 );
-		if( tmax >= 128 )
-		{
-			char const * tiling = getenv( "SPK_TILES" );
-			std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
-			                                                                       : balanced_tiles( segs, n, dev_sms, tmax, tmax_free );
-			if( (int)first.size() < spk::FLAT_PC )
-			{
-				// the largest tile with inputs sets the shared-memory floor (tiles without
-				// inputs need less than it per neuron)
-				int span = 0;
-				size_t si = 0;
-				for( size_t i = 0; i + 1 < first.size(); i++ )
-				{
-					while( si + 1 < segs.size() && segs[si + 1].start <= first[i] ) si++;
-					if( segs[si].cost > UPDATE_COST || first[i + 1] - first[i] <= tmax ) span = std::max( span, first[i + 1] - first[i] );
-				}
-				net.flat = true;
-				net.flat_tmax = ( span + 31 ) / 32 * 32;
-				net.tc = { spk::FLAT_THREADS, 1, net.flat_tmax, (int)first.size() - 1 };
-				set_tiles( net, first );
-			}
-		}
-	}
+	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.edges.alloc( (size_t)( n * width ) * 4 );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
@@ -804,6 +822,26 @@ void enqueue_pivots( spk_net & net )
 	if( net.flat ) build_slices( net );
 }
 
+// Re-tile a net that has not been stepped yet for about `target` tiles (batching): tiles,
+// pivots, slices and the per-tile buffers are rebuilt from the unchanged edges.
+void retile( spk_net & net, int target )
+{
+	require( net.steps == 0 && net.launched == 0, "a net is re-tiled before its first step" );
+	if( !net.flat ) return; // window_counts and window_plastic keep their fixed tiles
+	std::vector<cost_segment> segs;
+	for( size_t i = 0; i < net.seg_start.size(); i++ ) segs.push_back( { (long long)net.seg_start[i], net.seg_cost[i] } );
+	CK( cudaStreamSynchronize( net.stream ) );
+	require( flat_tiling( net, segs, target ), "tiling failed" );
+	net.pivots.alloc( (size_t)net.n * ( net.tc.ntiles + 1 ) * 4 );
+	net.ring_cnt.alloc( (size_t)2 * net.delay * net.tc.ntiles * 4 );
+	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
+	enqueue_pivots( net );
+	if( net.graph ) cudaGraphExecDestroy( net.graph );
+	net.graph = nullptr;
+	net.configure();
+	CK( cudaStreamSynchronize( net.stream ) );
+}
+
 void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned long long seed, int * d_edges, dbuf & conns_dev )
 {
 	std::vector<spk::conn_dev> cs;
@@ -835,6 +873,145 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	net->seed = seed;
 	CK( cudaStreamCreateWithFlags( &net->stream, cudaStreamNonBlocking ) );
 	return net.release();
+}
+} // namespace
+
+// ------------------------------------------------------------------------------------
+// batching: many independent window_flat nets stepped by shared launches
+// ------------------------------------------------------------------------------------
+struct spk_batch
+{
+	// the nets of one model: stepped by their own launches on their own stream, so the
+	// models' launches overlap
+	struct group
+	{
+		cudaStream_t stream = nullptr;
+		cudaEvent_t ev = nullptr;
+		dbuf d_params, d_jobs;
+		std::vector<spk::net_params> h_params;
+		std::vector<int4> h_jobs;
+	};
+	int device = 0;
+	std::vector<spk_net *> nets;
+	group groups[3]; // Vogels-Abbott, Brunel, synth
+
+	~spk_batch()
+	{
+		for( auto * net : nets ) net->batch = nullptr;
+		for( auto & g : groups )
+		{
+			if( g.ev ) cudaEventDestroy( g.ev );
+			if( g.stream ) cudaStreamDestroy( g.stream );
+		}
+	}
+
+	// stepped by the shared window_flat_batch launches
+	static bool shared( spk_net const & net ) { return net.flat && net.model != SPK_BRUNEL_PLUS; }
+	static int group_of( int model ) { return model == SPK_VOGELS_ABBOTT ? 0 : ( model == SPK_BRUNEL ? 1 : 2 ); }
+
+	template <typename Model>
+	static void launch_model( group & g, int4 const * jobs, int njobs, int smem )
+	{
+		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
+		{
+			spk::window_flat_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
+			CK( cudaGetLastError() );
+		}
+	}
+
+	// advance the nets of one model by nsteps: rounds of one launch, every tile of every net
+	// running up to its own window (delay) of steps per round
+	void run_group( group & g, int model, std::vector<spk_net *> const & gn, unsigned long long nsteps )
+	{
+		for( auto * net : gn )
+		{
+			net->flush();
+			CK( cudaEventRecord( g.ev, net->stream ) );
+			CK( cudaStreamWaitEvent( g.stream, g.ev, 0 ) );
+		}
+		g.h_params.resize( gn.size() );
+		for( size_t i = 0; i < gn.size(); i++ ) g.h_params[i] = gn[i]->params();
+		// all rounds' jobs (net, tile, steps, dt) at once; a round whose windows equal the
+		// previous round's reuses its jobs
+		std::vector<unsigned long long> left( gn.size(), nsteps );
+		std::vector<std::pair<int, int>> launches; // (first job, count)
+		g.h_jobs.clear();
+		std::vector<int> L( gn.size(), 0 ), prevL;
+		for( bool more = true; more; )
+		{
+			more = false;
+			for( size_t i = 0; i < gn.size(); i++ )
+				L[i] = left[i] ? (int)std::min<unsigned long long>( left[i], (unsigned long long)gn[i]->max_window() ) : 0;
+			if( L == prevL )
+				launches.push_back( launches.back() );
+			else
+			{
+				int const first = (int)g.h_jobs.size();
+				for( size_t i = 0; i < gn.size(); i++ )
+					if( L[i] )
+					{
+						int dtbits;
+						std::memcpy( &dtbits, &gn[i]->dt, 4 );
+						for( int j = 0; j < gn[i]->tc.ntiles; j++ ) g.h_jobs.push_back( make_int4( (int)i, j, L[i], dtbits ) );
+					}
+				launches.push_back( { first, (int)g.h_jobs.size() - first } );
+				prevL = L;
+			}
+			for( size_t i = 0; i < gn.size(); i++ )
+			{
+				left[i] -= L[i];
+				more = more || left[i];
+			}
+		}
+		size_t const pb = g.h_params.size() * sizeof( spk::net_params ), jb = g.h_jobs.size() * sizeof( int4 );
+		if( g.d_params.bytes < pb || g.d_jobs.bytes < jb ) CK( cudaStreamSynchronize( g.stream ) ); // launches reading the old ones
+		if( g.d_params.bytes < pb ) g.d_params.alloc( pb );
+		if( g.d_jobs.bytes < jb ) g.d_jobs.alloc( jb );
+		// pageable sources: each copy returns once its source is staged, and the stream
+		// orders it after the previous run's launches that read the same buffers
+		CK( cudaMemcpyAsync( g.d_params.p, g.h_params.data(), pb, cudaMemcpyHostToDevice, g.stream ) );
+		CK( cudaMemcpyAsync( g.d_jobs.p, g.h_jobs.data(), jb, cudaMemcpyHostToDevice, g.stream ) );
+		int const smem = gn[0]->flat_smem;
+		for( auto const & l : launches )
+		{
+			int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
+			switch( model )
+			{
+			case SPK_VOGELS_ABBOTT: launch_model<spice::vogels_abbott>( g, jobs, l.second, smem ); break;
+			case SPK_BRUNEL: launch_model<spice::brunel>( g, jobs, l.second, smem ); break;
+			case SPK_SYNTH: launch_model<spice::synth>( g, jobs, l.second, smem ); break;
+			}
+		}
+		for( auto * net : gn )
+		{
+			net->steps += nsteps;
+			net->launched += nsteps;
+		}
+		CK( cudaEventRecord( g.ev, g.stream ) );
+		for( auto * net : gn ) CK( cudaStreamWaitEvent( net->stream, g.ev, 0 ) );
+	}
+
+	void run( unsigned long long nsteps )
+	{
+		if( nets.empty() || nsteps == 0 ) return;
+		// nets outside window_flat (plastic ones) run their own windows on their own
+		// streams, concurrently with the shared launches
+		std::vector<spk_net *> gn[3];
+		for( auto * net : nets )
+			if( shared( *net ) ) gn[group_of( net->model )].push_back( net );
+			else net->run( nsteps );
+		int const models[3] = { SPK_VOGELS_ABBOTT, SPK_BRUNEL, SPK_SYNTH };
+		for( int m = 0; m < 3; m++ )
+			if( !gn[m].empty() ) run_group( groups[m], models[m], gn[m], nsteps );
+	}
+};
+
+namespace
+{
+void detach( spk_batch * b, spk_net * net )
+{
+	b->nets.erase( std::remove( b->nets.begin(), b->nets.end(), net ), b->nets.end() );
+	net->batch = nullptr;
 }
 } // namespace
 
@@ -967,6 +1144,7 @@ int spk_net_destroy( spk_net * net )
 {
 	return guarded( [&] {
 		if( !net ) return;
+		if( net->batch ) detach( net->batch, net );
 		{
 			device_guard g( net->device );
 			cudaStreamSynchronize( net->stream );
@@ -1258,4 +1436,77 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 		// cudaMemcpyAsync from pageable memory returns once the source has been staged, so
 		// the stack table may go out of scope while the copy and the kernel are in flight
 	} );
+}
+
+extern "C" {
+int spk_net_set_tile_target( spk_net * net, int target )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		require( target >= 1, "tile target must be >= 1" );
+		device_guard g( net->device );
+		retile( *net, target );
+	} );
+}
+
+int spk_batch_create( spk_batch ** out, int device )
+{
+	return guarded( [&] {
+		require( out != nullptr, "out is null" );
+		int ndev = 0;
+		CK( cudaGetDeviceCount( &ndev ) );
+		require( device >= 0 && device < ndev, "invalid device" );
+		device_guard g( device );
+		auto b = std::make_unique<spk_batch>();
+		b->device = device;
+		for( auto & g : b->groups )
+		{
+			CK( cudaStreamCreateWithFlags( &g.stream, cudaStreamNonBlocking ) );
+			CK( cudaEventCreateWithFlags( &g.ev, cudaEventDisableTiming ) );
+		}
+		*out = b.release();
+	} );
+}
+
+int spk_batch_add( spk_batch * b, spk_net * net )
+{
+	return guarded( [&] {
+		require( b != nullptr && net != nullptr, "null argument" );
+		require( net->device == b->device, "the net lives on another device" );
+		require( net->batch == nullptr, "the net belongs to a batch already" );
+		if( spk_batch::shared( *net ) )
+			for( auto * o : b->nets )
+				require( !spk_batch::shared( *o ) || o->flat_smem == net->flat_smem, "nets of a batch share one kernel configuration" );
+		b->nets.push_back( net );
+		net->batch = b;
+	} );
+}
+
+int spk_batch_remove( spk_batch * b, spk_net * net )
+{
+	return guarded( [&] {
+		require( b != nullptr && net != nullptr, "null argument" );
+		require( net->batch == b, "the net is not in the batch" );
+		detach( b, net );
+	} );
+}
+
+int spk_batch_run( spk_batch * b, uint64_t nsteps )
+{
+	return guarded( [&] {
+		require( b != nullptr, "batch is null" );
+		device_guard g( b->device );
+		b->run( nsteps );
+	} );
+}
+
+int spk_batch_destroy( spk_batch * b )
+{
+	return guarded( [&] {
+		if( !b ) return;
+		device_guard g( b->device );
+		for( auto & gr : b->groups ) cudaStreamSynchronize( gr.stream );
+		delete b;
+	} );
+}
 }

@@ -299,3 +299,76 @@ def test_persistent_run_matches_windows(model, pops, conns, delay, steps):
         assert bits_equal(x, y)
     for i in range(2 * delay):  # the spike ring the long launch left behind
         assert np.array_equal(a.step(out=True), b.step(out=True)), i
+
+
+# ----------------------------------------------------------------------- batching
+BATCH_NETS = [
+    ("vogels_abbott", [4000], [(0, 0, 0.02)], 8, 7),
+    ("vogels_abbott", [5000], [(0, 0, 0.02)], 1, 3),
+    ("brunel", [3000, 3000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 4),
+    ("brunel", [12000, 12000], [(0, 1, 0.05), (1, 1, 0.05)], 6, 20),
+    ("synth", [200_000], [(0, 0, 16 / 200_000)], 4, 12),
+    ("synth", [30_000], [(0, 0, 0.001)], 15, 1),
+    ("brunel_with_plasticity", [1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 2),  # own stream
+]
+
+
+def test_batch_matches_nets_alone():
+    """Nets of three models, uneven sizes and delays, re-tiled and stepped by shared
+    launches (and a plastic net beside them), against each net stepped alone: state
+    bit-identical, spikes equal."""
+    alone, batched = [], []
+    batch = spice_b200.Batch()
+    for i, (model, pops, conns, delay, target) in enumerate(BATCH_NETS):
+        layout = Layout(pops, conns)
+        alone.append(Snn(model, layout, delay=delay, seed=20 + i, graph_seed=40 + i))
+        b = Snn(model, layout, delay=delay, seed=20 + i, graph_seed=40 + i)
+        b.set_tile_target(target)
+        assert b.info().num_tiles <= alone[-1].info().num_tiles
+        batch.add(b)
+        batched.append(b)
+    # batch rounds, then steps with output on a batched net, then more rounds
+    batch.run(37)
+    for a in alone:
+        a.run(37)
+    for a, b in zip(alone, batched):
+        for k in range(3):
+            assert np.array_equal(a.step(out=True), b.step(out=True)), k
+    batch.run(101)
+    for a in alone:
+        a.run(101)
+    for a, b in zip(alone, batched):
+        assert a.info().steps == b.info().steps == 141
+        for x, y in zip(a.neurons(), b.neurons()):
+            assert bits_equal(x, y)
+        for x, y in zip(a.synapses(), b.synapses()):
+            assert bits_equal(x, y)
+        for k in range(2 * b.delay()):
+            assert np.array_equal(a.step(out=True), b.step(out=True)), k
+    batch.remove(batched[0])
+    batch.run(5)
+    assert batched[0].info().steps == 141 + 2 * batched[0].delay()
+    batched[1].close()  # a destroyed net leaves its batch
+    batch.run(2)
+    assert batched[2].info().steps == 141 + 2 * batched[2].delay() + 5 + 2
+    batch.close()
+
+
+def test_batch_rejects_stepped_retile_and_double_add():
+    batch = spice_b200.Batch()
+    n = Snn("brunel", Layout([500, 500], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15)
+    n.run(3)
+    with pytest.raises(spice_b200.InvalidArgument):
+        n.set_tile_target(4)
+    batch.add(n)
+    with pytest.raises(spice_b200.InvalidArgument):
+        batch.add(n)
+    other = spice_b200.Batch()
+    with pytest.raises(spice_b200.InvalidArgument):
+        other.add(n)
+    batch.run(4)
+    n.sync()
+    assert n.info().steps == 7
+    batch.close()
+    other.add(n)  # free again once its batch is gone
+    other.close()
