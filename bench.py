@@ -332,8 +332,9 @@ def tile_targets(specs, sms):
 def run_batched(args, rank, world):
     """Batched workload: the same nets stepped (a) one at a time, the plain per-job loop
     (spice_bench/paper_plots.cpp:184-231 steps one net after another), and (b) together in
-    one Batch. Setup is excluded from both; each arm's wall time is CUDA-event timed on the
-    device around its steps. Reports both and the ratio."""
+    one Batch. Setup is excluded from both; each arm's wall time is taken on the host from
+    an idle, synchronised GPU until every net has synchronised again (the batch spans many
+    streams). Reports both and the ratio."""
     import torch
 
     from spice_b200 import Batch, Layout, Snn
@@ -357,10 +358,13 @@ def run_batched(args, rank, world):
     torch.cuda.synchronize()
     clocks = Clocks(dev)
     clocks.start()
+    per_model = {m: 0.0 for m in BATCH_MODELS}
     t0 = time.perf_counter()
-    for n in plain:
+    for n, s in zip(plain, specs):
+        t = time.perf_counter()
         n.run(steps)
         n.sync()
+        per_model[s["model"]] += time.perf_counter() - t
     wall_plain = time.perf_counter() - t0
     syn_total = sum(n.num_synapses() for n in plain)
     for n in plain:
@@ -399,6 +403,7 @@ def run_batched(args, rank, world):
                            "syn_range": [1e5, 5e7], "bio_s_per_net": steps * DT, "dt": DT, "tiles_total": tiles},
                 "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch},
                 "plain_loop": {"wall_s": wall_plain, "wall_per_bio": wall_plain / bio_total, "setup_s": setup_plain,
+                               "wall_s_by_model": per_model,
                                "value": syn_total * steps * DT / wall_plain},
                 "speedup_vs_plain_loop": wall_plain / wall_batch, "clocks": clk}
         print(json.dumps(line), flush=True)

@@ -352,8 +352,16 @@ struct spk_net
 				persistent = coop && delay >= 6 && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
 				return;
 			}
+		// the limit is per kernel, shared by every net: set it to all a CTA can have, so a
+		// net configured later with smaller needs does not lower it under an earlier net's
 		with_window_kernel<Model>( [&]( auto kernel ) {
-			CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) );
+			int optin = 0;
+			CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
+			cudaFuncAttributes fa{};
+			CK( cudaFuncGetAttributes( &fa, kernel ) );
+			int const limit = optin - (int)fa.sharedSizeBytes;
+			require( smem <= limit, "shared memory too small for the tiling" );
+			CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit ) );
 		} );
 	}
 

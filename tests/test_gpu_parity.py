@@ -372,3 +372,17 @@ def test_batch_rejects_stepped_retile_and_double_add():
     batch.close()
     other.add(n)  # free again once its batch is gone
     other.close()
+
+
+@pytest.mark.parametrize("model,kernel", [("brunel_with_plasticity", None), ("brunel", "direct")])
+def test_nets_of_one_model_with_different_shared_memory(model, kernel, monkeypatch):
+    """A kernel's shared-memory limit is shared by all nets: a smaller net created after a
+    larger one must not break the larger one's launches."""
+    if kernel:
+        monkeypatch.setenv("SPK_KERNEL", kernel)
+    big = Snn(model, Layout([20_000, 20_000], [(0, 1, 0.02), (1, 1, 0.02)]), delay=15)
+    small = Snn(model, Layout([300, 300], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15)
+    big.run(30)
+    small.run(30)
+    big.sync()
+    small.sync()
