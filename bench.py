@@ -43,8 +43,13 @@ def parse():
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--syn", type=float, default=1e9,
                     help="total synapses of the Brunel net (the benchmark is 1e9; smaller sizes serve profiling)")
-    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched"],
-                    help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop")
+    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched", "serving"],
+                    help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop; "
+                         "serving: Poisson job arrivals, server vs plain per-job loop")
+    ap.add_argument("--duration", type=float, default=8.0, help="serving: seconds of job arrivals")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: job arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
+    ap.add_argument("--quantum", type=int, default=600, help="serving: steps per tick")
     ap.add_argument("--nets", type=int, default=256, help="batched: number of nets")
     ap.add_argument("--bio", type=float, default=1.0, help="batched: biological seconds per net")
     args = ap.parse_args()
@@ -409,6 +414,99 @@ def run_batched(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def serving_jobs(rate, duration, seed=0):
+    """Poisson arrivals at `rate` jobs/s over `duration` s; models uniform over {VA, Brunel,
+    Brunel+}, synapses log-uniform in 1e6-2e8, biological time uniform in 0.1-2 s."""
+    rng = np.random.default_rng(seed)
+    t, jobs = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration:
+            break
+        model = BATCH_MODELS[int(rng.integers(0, 3))]
+        syn = float(np.exp(rng.uniform(np.log(1e6), np.log(2e8))))
+        bio = float(rng.uniform(0.1, 2.0))
+        if model == "vogels_abbott":
+            n = int((syn / 0.02) ** 0.5)
+            pops, conns, delay = [n], [(0, 0, 0.02)], 8
+        else:
+            half = int((syn / 0.05) ** 0.5) // 2
+            pops, conns, delay = [half, half], [(0, 1, 0.1), (1, 1, 0.1)], 15
+        jobs.append({"t": t, "model": model, "pops": pops, "conns": conns, "delay": delay, "syn": syn,
+                     "steps": int(round(bio / DT)), "seed": len(jobs) + 1})
+    return jobs
+
+
+def run_serving(args, rank, world):
+    """Serving workload: the same seeded job arrivals served (a) by the plain per-job loop
+    (build, run and free one net at a time in arrival order, spice_bench/paper_plots.cpp:184-231)
+    and (b) by Server (admission against the budget, continuous batching). Latency = job
+    completion minus arrival; throughput = synapses x biological seconds of all jobs per wall
+    second from the first arrival to the last completion."""
+    import torch
+
+    from spice_b200 import Layout, Server, Snn
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    jobs = serving_jobs(args.rate, args.duration)
+    work = sum(j["syn"] * j["steps"] * DT for j in jobs)
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q)) if x else None
+
+    clocks = Clocks(dev)
+    clocks.start()
+    # (a) plain loop, real time
+    lat_plain = []
+    t0 = time.perf_counter()
+    for j in jobs:
+        now = time.perf_counter() - t0
+        if now < j["t"]:
+            time.sleep(j["t"] - now)
+        net = Snn(j["model"], Layout(j["pops"], j["conns"]), dt=DT, delay=j["delay"], seed=j["seed"],
+                  graph_seed=1000 + j["seed"], device=dev)
+        net.run(j["steps"])
+        net.sync()
+        net.close()
+        lat_plain.append(time.perf_counter() - t0 - j["t"])
+    span_plain = time.perf_counter() - t0
+
+    # (b) server, real time
+    srv = Server(budget_bytes=int(args.budget_gb * 1e9), quantum=args.quantum, device=dev)
+    ids = []
+    t0 = time.perf_counter()
+    for j in jobs:
+        now = time.perf_counter() - t0
+        if now < j["t"]:
+            time.sleep(j["t"] - now)
+        ids.append(srv.submit(j["model"], Layout(j["pops"], j["conns"]), j["steps"], dt=DT, delay=j["delay"],
+                              seed=j["seed"], graph_seed=1000 + j["seed"]))
+    srv.wait(timeout=1800)
+    infos = [srv.info(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    clk = clocks.stop()
+    states = [i.state for i in infos]
+    lat = [i.t_end - i.t_submit for i in infos if i.state == 2]
+    first = min(i.t_submit for i in infos)
+    span = max(i.t_end for i in infos) - first
+    if rank == 0:
+        counts = {m: sum(1 for j in jobs if j["model"] == m) for m in BATCH_MODELS}
+        line = {"metric": "served synapse-seconds per wall second", "value": work / span, "unit": "syn*bio_s/s",
+                "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": span * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"serving_poisson_{args.rate:g}_per_s", "jobs": len(jobs), "models": counts,
+                           "syn_range": [1e6, 2e8], "bio_range_s": [0.1, 2.0], "arrival_s": args.duration,
+                           "budget_gb": args.budget_gb, "quantum_steps": args.quantum},
+                "server": {"p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "span_s": span, "done": states.count(2),
+                           "peak_gb": st["peak_bytes"] / 1e9, "ticks": st["ticks"]},
+                "plain_loop": {"p50_s": pct(lat_plain, 50), "p99_s": pct(lat_plain, 99), "span_s": span_plain,
+                               "value": work / span_plain},
+                "speedup_vs_plain_loop": span_plain / span, "clocks": clk}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
@@ -417,6 +515,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "batched":
             run_batched(args, rank, world)
+        elif args.workload == "serving":
+            run_serving(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:

@@ -24,7 +24,8 @@ typedef enum spk_status
 	SPK_ERR_CUDA = 2,     /* CUDA runtime error (the reference throws std::runtime_error)    */
 	SPK_ERR_NOMEM = 3,    /* device allocation failed (the reference throws std::bad_alloc)  */
 	SPK_ERR_DEVICE = 4,   /* a kernel reported an error through the net's device error word */
-	SPK_ERR_CAPACITY = 5  /* an output buffer is too small; *count tells the size needed    */
+	SPK_ERR_CAPACITY = 5, /* an output buffer is too small; *count tells the size needed    */
+	SPK_ERR_TIMEOUT = 6   /* a host-side wait ran out (spk_server_wait)                      */
 } spk_status;
 
 typedef enum spk_model
@@ -115,6 +116,24 @@ int spk_net_create(
     uint64_t graph_seed,
     int device );
 
+/* spk_net_create with the number of window_flat tiles chosen for about `tile_target`
+ * (0 = one per SM, the default): a net that shares the GPU with others (a batch, a server)
+ * takes fewer CTAs. Results do not depend on the tiling. */
+int spk_net_create_ex(
+    spk_net ** out,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    int device,
+    int tile_target );
+
+/* Upper estimate of the device memory (bytes) a net of this model, layout, delay and tile
+ * target would hold once built: what a server admits against its memory budget. */
+int spk_net_estimate_bytes( int model, spk_layout_desc const * desc, int delay, int device, int tile_target, uint64_t * out_bytes );
+
 /* cuda::snn<Model>(adj, width, dt, delay) (spice/cuda/snn.h:26-32, spice/cuda/snn.d.cpp:167-199):
  * imports an ELL adjacency (num_neurons x width int32, rows ascending, INT_MAX padded,
  * width a multiple of 32) from host memory and initialises neurons and synapses. */
@@ -198,7 +217,82 @@ int spk_batch_remove( spk_batch * batch, spk_net * net );
  * the launches; each net's own stream is ordered after them, so spk_net_sync and the
  * state exports of a net see the batch's steps). */
 int spk_batch_run( spk_batch * batch, uint64_t nsteps );
+/* Advance nets[i] (members of the batch, each listed once) by nsteps[i] steps. */
+int spk_batch_run_nets( spk_batch * batch, int count, spk_net * const * nets, uint64_t const * nsteps );
 int spk_batch_destroy( spk_batch * batch );
+
+/* ---- serving: jobs admitted against a device-memory budget, continuously batched ----
+ * A server owns one worker thread and one batch on `device`. Submitted jobs queue in
+ * arrival order; the head is admitted when its estimated device memory
+ * (spk_net_estimate_bytes) fits the budget beside the running jobs, and its net is built
+ * with a tile count sized to its share of the load. Every tick advances each running job
+ * by up to `quantum_steps` steps in one batch run; jobs admitted meanwhile join the next
+ * tick. A completed job's final neuron state is kept in host memory (same values as the
+ * net stepped alone) and its device memory is freed at once. */
+typedef struct spk_server spk_server;
+
+typedef enum spk_job_state
+{
+	SPK_JOB_QUEUED = 0,
+	SPK_JOB_RUNNING = 1,
+	SPK_JOB_DONE = 2,
+	SPK_JOB_FAILED = 3,    /* building or stepping failed: error and message say why   */
+	SPK_JOB_CANCELLED = 4,
+	SPK_JOB_TIMEOUT = 5,   /* the job's deadline passed before it completed            */
+	SPK_JOB_REFUSED = 6    /* larger than the whole budget: refused at submission      */
+} spk_job_state;
+
+typedef struct spk_job_info
+{
+	int state;             /* spk_job_state                                             */
+	int error;             /* spk_status of a failed or refused job                     */
+	uint64_t steps_done;
+	uint64_t steps_total;
+	uint64_t num_neurons;  /* of a completed job (its state's length)                  */
+	uint64_t device_bytes; /* held against the budget while queued for admission / running */
+	double t_submit;       /* seconds since the server was created                      */
+	double t_start;        /* admission (-1 before)                                     */
+	double t_end;          /* completion, failure, cancellation or timeout (-1 before)  */
+	char message[160];
+} spk_job_info;
+
+typedef struct spk_server_stats
+{
+	uint64_t queued, running, done, failed, cancelled, timed_out, refused;
+	uint64_t bytes_in_use, peak_bytes, budget_bytes;
+	uint64_t ticks;
+} spk_server_stats;
+
+int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps );
+/* Queue a job: the arguments of spk_net_create, its number of steps and a deadline in
+ * seconds from submission (0 = none). SPK_ERR_NOMEM (and a job in state REFUSED) if the
+ * job alone exceeds the budget. */
+int spk_server_submit(
+    spk_server * server,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    uint64_t nsteps,
+    double timeout_s,
+    uint64_t * out_job );
+int spk_server_job_info( spk_server * server, uint64_t job, spk_job_info * out );
+/* Final neuron state of a completed job, one host array per attribute (spk_model_attrs). */
+int spk_server_job_neurons( spk_server * server, uint64_t job, void * const * attrs );
+int spk_server_cancel( spk_server * server, uint64_t job );
+/* Forget a finished job (frees its host results). */
+int spk_server_release( spk_server * server, uint64_t job );
+/* Block until `job` (0 = every job) is finished; timeout_s < 0 waits without limit,
+ * otherwise SPK_ERR_TIMEOUT when it runs out. */
+int spk_server_wait( spk_server * server, uint64_t job, double timeout_s );
+int spk_server_get_stats( spk_server * server, spk_server_stats * out );
+/* Fault injection on the host: the next `count` admissions fail as an allocation failure
+ * would (the job ends FAILED with SPK_ERR_NOMEM; the server carries on). */
+int spk_server_inject_alloc_failures( spk_server * server, int count );
+/* Stops the worker; running jobs are dropped. */
+int spk_server_destroy( spk_server * server );
 
 #ifdef __cplusplus
 }

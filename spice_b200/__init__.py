@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(_HERE, "libspice_b200.so")
 MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3}
 MODEL_NAMES = {v: k for k, v in MODELS.items()}
 
-OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_DEVICE, ERR_CAPACITY = range(6)
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_DEVICE, ERR_CAPACITY, ERR_TIMEOUT = range(7)
 
 
 class SpiceError(RuntimeError):
@@ -68,6 +68,28 @@ class NetInfo(C.Structure):
     ]
 
 
+class JobInfo(C.Structure):  # spk_job_info
+    _fields_ = [
+        ("state", C.c_int),
+        ("error", C.c_int),
+        ("steps_done", C.c_uint64),
+        ("steps_total", C.c_uint64),
+        ("num_neurons", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("t_submit", C.c_double),
+        ("t_start", C.c_double),
+        ("t_end", C.c_double),
+        ("message", C.c_char * 160),
+    ]
+
+
+class ServerStats(C.Structure):  # spk_server_stats
+    _fields_ = [(k, C.c_uint64) for k in ("queued", "running", "done", "failed", "cancelled", "timed_out", "refused",
+                                          "bytes_in_use", "peak_bytes", "budget_bytes", "ticks")]
+
+
+JOB_STATES = ("queued", "running", "done", "failed", "cancelled", "timeout", "refused")
+
 _lib = None
 
 
@@ -101,6 +123,19 @@ def library():
         "spk_net_synapses": (I, [VP, P(VP)]),
         "spk_model_attrs": (I, [I, P(I), P(I), C.c_char_p, I]),
         "spk_net_set_tile_target": (I, [VP, I]),
+        "spk_net_create_ex": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I, I]),
+        "spk_net_estimate_bytes": (I, [I, P(_LayoutDesc), I, I, I, P(U64)]),
+        "spk_batch_run_nets": (I, [VP, I, P(VP), P(U64)]),
+        "spk_server_create": (I, [P(VP), I, U64, U64]),
+        "spk_server_submit": (I, [VP, I, P(_LayoutDesc), F, I, U64, U64, U64, C.c_double, P(U64)]),
+        "spk_server_job_info": (I, [VP, U64, P(JobInfo)]),
+        "spk_server_job_neurons": (I, [VP, U64, P(VP)]),
+        "spk_server_cancel": (I, [VP, U64]),
+        "spk_server_release": (I, [VP, U64]),
+        "spk_server_wait": (I, [VP, U64, C.c_double]),
+        "spk_server_get_stats": (I, [VP, P(ServerStats)]),
+        "spk_server_inject_alloc_failures": (I, [VP, I]),
+        "spk_server_destroy": (I, [VP]),
         "spk_batch_create": (I, [P(VP), I]),
         "spk_batch_add": (I, [VP, VP]),
         "spk_batch_remove": (I, [VP, VP]),
@@ -363,6 +398,93 @@ class Batch:
             _check(library().spk_batch_destroy(self._h))
             self._h = C.c_void_p()
             self._nets = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def estimate_bytes(model, layout, delay=1, device=0, tile_target=0):
+    """Upper estimate of the device memory a net of this model and layout would hold."""
+    m = MODELS[model] if isinstance(model, str) else int(model)
+    d = layout.desc()
+    out = C.c_uint64()
+    _check(library().spk_net_estimate_bytes(m, C.byref(d), int(delay), int(device), int(tile_target), C.byref(out)))
+    return out.value
+
+
+class Server:
+    """Simulation jobs admitted against a device-memory budget and stepped by continuous
+    batching on one GPU (a native worker thread; see spk_server_* in spice_b200.h).
+
+    srv = Server(budget_bytes=150e9, quantum=1500)
+    job = srv.submit("brunel", layout, nsteps=10_000, delay=15, seed=1)
+    srv.wait(job); V, Twait = srv.neurons(job)
+    """
+
+    def __init__(self, budget_bytes, quantum=1500, device=0):
+        self._h = C.c_void_p()
+        self._models = {}
+        _check(library().spk_server_create(C.byref(self._h), int(device), int(budget_bytes), int(quantum)))
+
+    def submit(self, model, layout, nsteps, dt=1e-4, delay=1, seed=1, graph_seed=1337, timeout=0.0):
+        """Queue a job; returns its id. Raises SpiceError (ERR_NOMEM) if it alone exceeds the budget."""
+        name = model if isinstance(model, str) else MODEL_NAMES[int(model)]
+        d = layout.desc()
+        job = C.c_uint64()
+        code = library().spk_server_submit(self._h, MODELS[name], C.byref(d), float(dt), int(delay), int(seed),
+                                           int(graph_seed), int(nsteps), float(timeout), C.byref(job))
+        self._models[job.value] = name
+        _check(code)
+        return job.value
+
+    def info(self, job):
+        i = JobInfo()
+        _check(library().spk_server_job_info(self._h, int(job), C.byref(i)))
+        return i
+
+    def state(self, job):
+        return JOB_STATES[self.info(job).state]
+
+    def neurons(self, job):
+        """Final neuron state of a completed job (one array per attribute)."""
+        i = self.info(job)
+        ndt, _ = model_attrs(self._models[int(job)])
+        arrs = [np.empty(i.num_neurons, dtype=t) for t in ndt]
+        _check(library().spk_server_job_neurons(self._h, int(job), _arr_ptrs(arrs)))
+        return arrs
+
+    def cancel(self, job):
+        _check(library().spk_server_cancel(self._h, int(job)))
+
+    def release(self, job):
+        _check(library().spk_server_release(self._h, int(job)))
+        self._models.pop(int(job), None)
+
+    def wait(self, job=0, timeout=-1.0):
+        """Block until `job` (0 = all jobs) is finished; raises SpiceError(ERR_TIMEOUT) if timeout runs out."""
+        _check(library().spk_server_wait(self._h, int(job), float(timeout)))
+
+    def stats(self):
+        st = ServerStats()
+        _check(library().spk_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def inject_alloc_failures(self, count):
+        _check(library().spk_server_inject_alloc_failures(self._h, int(count)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(library().spk_server_destroy(self._h))
+            self._h = C.c_void_p()
 
     def __del__(self):
         try:

@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspice_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "net.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "net.cu"), os.path.join(HERE, "csrc", "server.cpp")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "plastic.cuh", "flat.cuh", "device_common.cuh")]
 
 
@@ -34,7 +34,7 @@ def command(out=LIB, extra=()):
         "-lineinfo", "-O3", "-std=c++17",
         "-fmad=false",
         "--expt-relaxed-constexpr",
-        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-pthread",
         "-shared",
         "-I", os.path.join(ROOT, "include"),
         "-o", out,

@@ -146,6 +146,9 @@ model_desc describe( int model )
 	}
 }
 
+int classes_of( int model ) { return model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 ); }
+int neuron_attrs_of( int model ) { return model == SPK_VOGELS_ABBOTT ? 4 : ( model == SPK_SYNTH ? 1 : 2 ); }
+
 spice::util::layout to_layout( spk_layout_desc const * d )
 {
 	require( d != nullptr, "layout descriptor is null" );
@@ -283,8 +286,8 @@ struct spk_net
 		return b;
 	}
 
-	int classes() const { return model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 ); }
-	int neuron_attrs() const { return model == SPK_VOGELS_ABBOTT ? 4 : ( model == SPK_SYNTH ? 1 : 2 ); }
+	int classes() const { return classes_of( model ); }
+	int neuron_attrs() const { return neuron_attrs_of( model ); }
 
 	int window_smem() const
 	{
@@ -675,36 +678,45 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 	CK( cudaMemcpy( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice ) );
 }
 
-// window_flat's tiling of a net into at most about `target` work-balanced tiles (target =
-// the SM count for a net alone; fewer for a net that shares the GPU in a batch). Sets
-// net.flat and the tiles; false if the net does not fit window_flat.
-bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int target )
+// window_flat's tiling of n neurons into at most about `target` work-balanced tiles (target
+// = the SM count for a net alone; fewer for a net that shares the GPU in a batch): the
+// tiles' first neurons and the shared-memory span of the largest tile with inputs; false
+// if the net does not fit window_flat.
+bool plan_flat( int model, int device, long long n, std::vector<cost_segment> const & segs, int target, std::vector<int> & first, int & span )
 {
-	long long const n = net.n;
 	int optin = 0;
-	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net.device ) );
+	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
+	int const classes = classes_of( model ), attrs = neuron_attrs_of( model );
 	// largest tile whose counters, state, tables and minimal slice ring fit (with room for
 	// the kernel's static shared memory), and whose counter indices fit 16 bits
 	int tmax = spk::FLAT_MAX_TILE;
-	while( tmax >= 128 && ( spk::flat_smem_bytes( net.classes(), net.neuron_attrs(), tmax ) + 4096 > (size_t)optin ||
-	                        (long long)net.classes() * tmax >= spk::SLICE_PAD ) )
+	while( tmax >= 128 && ( spk::flat_smem_bytes( classes, attrs, tmax ) + 4096 > (size_t)optin || (long long)classes * tmax >= spk::SLICE_PAD ) )
 		tmax -= 32;
 	// tiles without inputs keep only their neuron state and fired bits
-	int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * net.neuron_attrs() + 8 ) ) / 32 * 32 );
+	int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * attrs + 8 ) ) / 32 * 32 );
 	if( tmax < 128 ) return false;
 	char const * tiling = getenv( "SPK_TILES" );
-	std::vector<int> const first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
-	                                                                       : balanced_tiles( segs, n, std::max( 1, target ), tmax, tmax_free );
+	first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
+	                                                   : balanced_tiles( segs, n, std::max( 1, target ), tmax, tmax_free );
 	if( (int)first.size() >= spk::FLAT_PC ) return false;
 	// the largest tile with inputs sets the shared-memory floor (tiles without inputs need
 	// less than it per neuron)
-	int span = 0;
+	span = 0;
 	size_t si = 0;
 	for( size_t i = 0; i + 1 < first.size(); i++ )
 	{
 		while( si + 1 < segs.size() && segs[si + 1].start <= first[i] ) si++;
 		if( segs[si].cost > UPDATE_COST || first[i + 1] - first[i] <= tmax ) span = std::max( span, first[i + 1] - first[i] );
 	}
+	return true;
+}
+
+// plan_flat applied to a net: sets net.flat and the tiles
+bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int target )
+{
+	std::vector<int> first;
+	int span = 0;
+	if( !plan_flat( net.model, net.device, net.n, segs, target, first, span ) ) return false;
 	net.flat = true;
 	net.flat_tmax = ( span + 31 ) / 32 * 32;
 	net.tc = { spk::FLAT_THREADS, 1, net.flat_tmax, (int)first.size() - 1 };
@@ -713,7 +725,7 @@ bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int tar
 }
 
 // buffers + pivots; edges must be filled before build_pivots is enqueued
-void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs )
+void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs, int tile_target = 0 )
 {
 	require( n > 0 && n <= INT_MAX, "invalid neuron count" );
 	require( width >= 0 && width % 32 == 0, "width must be a multiple of 32" );
@@ -737,7 +749,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	}
 	net.flat = false;
 	char const * kern = getenv( "SPK_KERNEL" );
-	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, dev_sms );
+	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, tile_target > 0 ? tile_target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.edges.alloc( (size_t)( n * width ) * 4 );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
@@ -864,6 +876,73 @@ void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned l
 	CK( cudaGetLastError() );
 }
 
+// Upper estimate of the device memory a net of this layout holds once built (the buffers
+// of allocate, build_slices and the plastic state; slices bounded by one 16-byte vector per
+// eight synapses plus one per non-empty (source, tile) pair, at 5 % above the expected
+// synapse count), each buffer rounded up to the allocator's 2 MiB granule.
+size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int device, int tile_target )
+{
+	long long const n = (long long)l.size(), w = (long long)l.max_degree();
+	double syn = 0;
+	for( auto const & c : l.connections() )
+		syn += (double)( std::get<1>( c ) - std::get<0>( c ) ) * (double)( std::get<3>( c ) - std::get<2>( c ) ) * std::get<4>( c );
+	syn = std::min( syn * 1.05, (double)n * w );
+	int sms = 0;
+	CK( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ) );
+	int const attrs = describe( model ).neuron_attrs;
+	bool flat = false;
+	long long T = 0;
+	if( model != SPK_BRUNEL_PLUS )
+	{
+		std::vector<int> first;
+		int span = 0;
+		char const * kern = getenv( "SPK_KERNEL" );
+		if( !( kern && !strcmp( kern, "direct" ) ) && plan_flat( model, device, n, layout_costs( l ), tile_target > 0 ? tile_target : sms, first, span ) )
+		{
+			flat = true;
+			T = (long long)first.size() - 1;
+		}
+		else
+			T = choose_tiles( n, sms, 2048, 4 ).ntiles;
+	}
+	else
+		T = choose_tiles( n, sms, 512, 1 ).ntiles;
+	std::vector<double> b = { (double)n * w * 4,
+	                          (double)n * ( T + 1 ) * 4,
+	                          2.0 * delay * n * 4,
+	                          2.0 * delay * T * 4,
+	                          64,
+	                          spk::DT_RING * 4.0,
+	                          4,
+	                          (double)n * 4,
+	                          4,
+	                          8,
+	                          4,
+	                          4096 };
+	for( int i = 0; i < attrs; i++ ) b.push_back( (double)n * 4 );
+	if( flat )
+	{
+		b.push_back( (double)n * T * 8 );
+		b.push_back( 16.0 * ( std::ceil( syn / 8 ) + std::min( (double)n * T, syn ) ) );
+		b.push_back( (double)T * 8 );
+		b.push_back( (double)T * 4 );
+	}
+	if( model == SPK_BRUNEL_PLUS )
+	{
+		b.push_back( (double)n * w * 4 );
+		for( int i = 0; i < 8; i++ ) b.push_back( (double)n * 4 );
+		b.push_back( (double)n * 8 );
+		b.push_back( 2.0 * delay * n * 16 );
+		b.push_back( 2.0 * delay * n * 16 );
+		b.push_back( 2.0 * delay * T * 4 );
+		b.push_back( 2.0 * delay * T * 4 );
+	}
+	double const granule = 2.0 * 1024 * 1024;
+	double total = 0;
+	for( double x : b ) total += std::ceil( x / granule ) * granule;
+	return (size_t)total;
+}
+
 spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int device )
 {
 	describe( model );
@@ -929,7 +1008,7 @@ struct spk_batch
 
 	// advance the nets of one model by nsteps: rounds of one launch, every tile of every net
 	// running up to its own window (delay) of steps per round
-	void run_group( group & g, int model, std::vector<spk_net *> const & gn, unsigned long long nsteps )
+	void run_group( group & g, int model, std::vector<spk_net *> const & gn, std::vector<unsigned long long> const & counts )
 	{
 		for( auto * net : gn )
 		{
@@ -941,11 +1020,11 @@ struct spk_batch
 		for( size_t i = 0; i < gn.size(); i++ ) g.h_params[i] = gn[i]->params();
 		// all rounds' jobs (net, tile, steps, dt) at once; a round whose windows equal the
 		// previous round's reuses its jobs
-		std::vector<unsigned long long> left( gn.size(), nsteps );
+		std::vector<unsigned long long> left = counts;
 		std::vector<std::pair<int, int>> launches; // (first job, count)
 		g.h_jobs.clear();
 		std::vector<int> L( gn.size(), 0 ), prevL;
-		for( bool more = true; more; )
+		for( bool more = std::any_of( left.begin(), left.end(), []( unsigned long long x ) { return x > 0; } ); more; )
 		{
 			more = false;
 			for( size_t i = 0; i < gn.size(); i++ )
@@ -990,27 +1069,36 @@ struct spk_batch
 			case SPK_SYNTH: launch_model<spice::synth>( g, jobs, l.second, smem ); break;
 			}
 		}
-		for( auto * net : gn )
+		for( size_t i = 0; i < gn.size(); i++ )
 		{
-			net->steps += nsteps;
-			net->launched += nsteps;
+			gn[i]->steps += counts[i];
+			gn[i]->launched += counts[i];
 		}
 		CK( cudaEventRecord( g.ev, g.stream ) );
 		for( auto * net : gn ) CK( cudaStreamWaitEvent( net->stream, g.ev, 0 ) );
 	}
 
-	void run( unsigned long long nsteps )
+	// advance nets[i] by counts[i] steps (members of the batch)
+	void run( std::vector<spk_net *> const & which, std::vector<unsigned long long> const & counts )
 	{
-		if( nets.empty() || nsteps == 0 ) return;
 		// nets outside window_flat (plastic ones) run their own windows on their own
 		// streams, concurrently with the shared launches
 		std::vector<spk_net *> gn[3];
-		for( auto * net : nets )
-			if( shared( *net ) ) gn[group_of( net->model )].push_back( net );
-			else net->run( nsteps );
+		std::vector<unsigned long long> gc[3];
+		for( size_t i = 0; i < which.size(); i++ )
+		{
+			if( counts[i] == 0 ) continue;
+			if( shared( *which[i] ) )
+			{
+				gn[group_of( which[i]->model )].push_back( which[i] );
+				gc[group_of( which[i]->model )].push_back( counts[i] );
+			}
+			else
+				which[i]->run( counts[i] );
+		}
 		int const models[3] = { SPK_VOGELS_ABBOTT, SPK_BRUNEL, SPK_SYNTH };
 		for( int m = 0; m < 3; m++ )
-			if( !gn[m].empty() ) run_group( groups[m], models[m], gn[m], nsteps );
+			if( !gn[m].empty() ) run_group( groups[m], models[m], gn[m], gc[m] );
 	}
 };
 
@@ -1022,6 +1110,8 @@ void detach( spk_batch * b, spk_net * net )
 	net->batch = nullptr;
 }
 } // namespace
+
+void spk_set_last_error( std::string const & msg ) { g_err = msg; }
 
 extern "C" {
 char const * spk_last_error( void ) { return g_err.c_str(); }
@@ -1067,18 +1157,36 @@ int spk_generate_adj_list( void * stream, spk_layout_desc const * desc, uint64_t
 
 int spk_net_create( spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device )
 {
+	return spk_net_create_ex( out, model, desc, dt, delay, seed, graph_seed, device, 0 );
+}
+
+int spk_net_create_ex(
+    spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target )
+{
 	return guarded( [&] {
 		require( out != nullptr, "out is null" );
+		require( tile_target >= 0, "tile target must be >= 0" );
 		*out = nullptr;
 		auto const l = to_layout( desc );
 		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
 		device_guard g( device );
-		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ) );
+		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ), tile_target );
 		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev );
 		enqueue_pivots( *net );
 		init_state( *net );
 		CK( cudaStreamSynchronize( net->stream ) );
 		*out = net.release();
+	} );
+}
+
+int spk_net_estimate_bytes( int model, spk_layout_desc const * desc, int delay, int device, int tile_target, uint64_t * out_bytes )
+{
+	return guarded( [&] {
+		require( out_bytes != nullptr, "out is null" );
+		require( delay >= 1 && tile_target >= 0, "invalid delay or tile target" );
+		describe( model );
+		auto const l = to_layout( desc );
+		*out_bytes = estimate_bytes( model, l, delay, device, tile_target );
 	} );
 }
 
@@ -1504,7 +1612,22 @@ int spk_batch_run( spk_batch * b, uint64_t nsteps )
 	return guarded( [&] {
 		require( b != nullptr, "batch is null" );
 		device_guard g( b->device );
-		b->run( nsteps );
+		b->run( b->nets, std::vector<unsigned long long>( b->nets.size(), nsteps ) );
+	} );
+}
+
+int spk_batch_run_nets( spk_batch * b, int count, spk_net * const * nets, uint64_t const * nsteps )
+{
+	return guarded( [&] {
+		require( b != nullptr, "batch is null" );
+		require( count >= 0 && ( count == 0 || ( nets && nsteps ) ), "bad net arrays" );
+		std::vector<spk_net *> which( nets, nets + count );
+		for( auto * n : which ) require( n != nullptr && n->batch == b, "a net is not in the batch" );
+		std::vector<spk_net *> sorted = which;
+		std::sort( sorted.begin(), sorted.end() );
+		require( std::adjacent_find( sorted.begin(), sorted.end() ) == sorted.end(), "a net is listed twice" );
+		device_guard g( b->device );
+		b->run( which, std::vector<unsigned long long>( nsteps, nsteps + count ) );
 	} );
 }
 

@@ -1,0 +1,485 @@
+// Serving loop: simulation jobs submitted at any time, admitted against a device-memory
+// budget, stepped together by continuous batching.
+//
+// The reference has no server; a workload of many nets is a host loop that builds and steps
+// one net after another (spice_bench/paper_plots.cpp:184-231). Here one worker thread per
+// server owns the GPU side:
+//   admit   queued jobs in arrival order while their estimated device memory fits the
+//           budget (a job larger than the whole budget is refused at submission); each
+//           admitted job's net is built with a tile count sized to its share of the load;
+//   tick    every running job advances by up to `quantum` steps in one batch run (jobs
+//           admitted since the last tick join it: continuous batching);
+//   retire  finished jobs export their final neuron state to host memory and free their
+//           device memory; cancelled, timed-out and failed jobs free theirs too.
+// The server is a client of the C ABI only (spk_net_*, spk_batch_*): a job's results are
+// those of the same net stepped alone.
+#include <spice_b200.h>
+
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+// the library's per-thread error message (spk_last_error), defined with the C ABI
+void spk_set_last_error( std::string const & msg );
+
+namespace
+{
+int fail( int code, std::string const & msg )
+{
+	spk_set_last_error( msg );
+	return code;
+}
+
+struct job
+{
+	uint64_t id = 0;
+	int model = 0;
+	std::vector<uint64_t> pops;
+	std::vector<int> src, dst;
+	std::vector<float> p;
+	float dt = 0;
+	int delay = 1;
+	uint64_t seed = 0, graph_seed = 0, nsteps = 0;
+	double timeout_s = 0;
+
+	int state = SPK_JOB_QUEUED;
+	int error = SPK_OK;
+	std::string message;
+	uint64_t done = 0;
+	uint64_t reserved = 0; // device bytes held against the budget
+	uint64_t num_neurons = 0;
+	double t_submit = 0, t_start = -1, t_end = -1;
+	bool cancel = false;
+	spk_net * net = nullptr;
+	double work = 0;                           // expected cost per step (tiling share)
+	std::vector<std::vector<uint32_t>> result; // final neuron attributes (4-byte words)
+
+	spk_layout_desc desc() const
+	{
+		return { (int)pops.size(), pops.data(), (int)src.size(), src.data(), dst.data(), p.data() };
+	}
+	bool final() const { return state >= SPK_JOB_DONE; }
+};
+
+struct server
+{
+	int device = 0;
+	uint64_t budget = 0, quantum = 0;
+	int sms = 148;
+	spk_batch * batch = nullptr;
+	std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+	std::mutex mu;
+	std::condition_variable wake, changed;
+	bool stop = false;
+	uint64_t next_id = 1;
+	std::map<uint64_t, std::unique_ptr<job>> jobs;
+	std::deque<job *> queue;
+	std::vector<job *> running;
+	uint64_t in_use = 0, peak = 0, ticks = 0;
+	int inject = 0;
+	std::thread worker;
+
+	double now() const { return std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count(); }
+
+	void finish( job & j, int state, int error = SPK_OK, std::string const & msg = {} )
+	{
+		j.state = state;
+		j.error = error;
+		j.message = msg;
+		j.t_end = now();
+		changed.notify_all();
+	}
+
+	// tile target of a new job: its share of the SMs by expected work against the jobs
+	// already running (one tile at least)
+	int tile_target( job const & j ) const
+	{
+		double total = j.work;
+		for( auto * r : running ) total += r->work;
+		return std::max( 1, (int)std::lround( sms * j.work / total ) );
+	}
+
+	// build the net of an admitted job (lock not held)
+	int build( job & j, int target, std::string & msg )
+	{
+		auto const d = j.desc();
+		int rc = spk_net_create_ex( &j.net, j.model, &d, j.dt, j.delay, j.seed, j.graph_seed, device, target );
+		if( rc == SPK_OK ) rc = spk_batch_add( batch, j.net );
+		if( rc != SPK_OK )
+		{
+			msg = spk_last_error();
+			if( j.net ) spk_net_destroy( j.net );
+			j.net = nullptr;
+		}
+		return rc;
+	}
+
+	void loop()
+	{
+		std::unique_lock<std::mutex> lk( mu );
+		while( !stop )
+		{
+			double const t = now();
+			// queued jobs: cancellations and deadlines
+			for( auto it = queue.begin(); it != queue.end(); )
+			{
+				job & j = **it;
+				if( j.cancel || ( j.timeout_s > 0 && t - j.t_submit > j.timeout_s ) )
+				{
+					finish( j, j.cancel ? SPK_JOB_CANCELLED : SPK_JOB_TIMEOUT );
+					it = queue.erase( it );
+				}
+				else
+					++it;
+			}
+			// admission in arrival order while the head fits the budget
+			while( !queue.empty() && in_use + queue.front()->reserved <= budget && !stop )
+			{
+				job & j = *queue.front();
+				queue.pop_front();
+				in_use += j.reserved;
+				peak = std::max( peak, in_use );
+				j.state = SPK_JOB_RUNNING;
+				j.t_start = now();
+				int const target = tile_target( j );
+				bool const injected = inject > 0;
+				if( injected ) inject--;
+				lk.unlock();
+				std::string msg;
+				int const rc = injected ? ( msg = "injected allocation failure", SPK_ERR_NOMEM ) : build( j, target, msg );
+				lk.lock();
+				if( rc != SPK_OK )
+				{
+					in_use -= j.reserved;
+					j.reserved = 0;
+					finish( j, SPK_JOB_FAILED, rc, msg );
+					continue;
+				}
+				running.push_back( &j );
+			}
+			if( running.empty() )
+			{
+				wake.wait_for( lk, std::chrono::milliseconds( 20 ) );
+				continue;
+			}
+			// one tick: every running job up to `quantum` steps
+			std::vector<spk_net *> nets;
+			std::vector<uint64_t> counts;
+			std::vector<job *> ticked;
+			for( auto * j : running )
+				if( !j->cancel && j->done < j->nsteps )
+				{
+					nets.push_back( j->net );
+					counts.push_back( std::min( quantum, j->nsteps - j->done ) );
+					ticked.push_back( j );
+				}
+			lk.unlock();
+			std::vector<int> status( ticked.size(), SPK_OK );
+			std::vector<std::string> msgs( ticked.size() );
+			int rc = nets.empty() ? SPK_OK : spk_batch_run_nets( batch, (int)nets.size(), nets.data(), counts.data() );
+			std::string const run_msg = rc != SPK_OK ? spk_last_error() : "";
+			for( size_t i = 0; i < ticked.size(); i++ )
+			{
+				status[i] = rc != SPK_OK ? rc : spk_net_sync( nets[i] );
+				if( status[i] != SPK_OK ) msgs[i] = rc != SPK_OK ? run_msg : spk_last_error();
+			}
+			lk.lock();
+			ticks++;
+			for( size_t i = 0; i < ticked.size(); i++ )
+				if( status[i] == SPK_OK ) ticked[i]->done += counts[i];
+			// retire: finished, failed, cancelled and timed-out jobs
+			double const te = now();
+			std::vector<std::pair<job *, int>> leaving; // (job, final state)
+			std::vector<int> errs;
+			std::vector<std::string> emsgs;
+			for( auto it = running.begin(); it != running.end(); )
+			{
+				job & j = **it;
+				auto const k = std::find( ticked.begin(), ticked.end(), &j ) - ticked.begin();
+				int const st = (size_t)k < ticked.size() ? status[k] : SPK_OK;
+				int state = -1;
+				if( st != SPK_OK ) state = SPK_JOB_FAILED;
+				else if( j.done >= j.nsteps ) state = SPK_JOB_DONE;
+				else if( j.cancel ) state = SPK_JOB_CANCELLED;
+				else if( j.timeout_s > 0 && te - j.t_submit > j.timeout_s ) state = SPK_JOB_TIMEOUT;
+				if( state < 0 )
+				{
+					++it;
+					continue;
+				}
+				leaving.push_back( { &j, state } );
+				errs.push_back( st );
+				emsgs.push_back( (size_t)k < ticked.size() ? msgs[k] : std::string() );
+				it = running.erase( it );
+			}
+			lk.unlock();
+			for( size_t i = 0; i < leaving.size(); i++ )
+			{
+				job & j = *leaving[i].first;
+				if( leaving[i].second == SPK_JOB_DONE )
+				{
+					spk_net_info info{};
+					int na = 0, ns = 0;
+					char types[16];
+					int r = spk_net_get_info( j.net, &info );
+					if( r == SPK_OK ) r = spk_model_attrs( j.model, &na, &ns, types, sizeof types );
+					std::vector<std::vector<uint32_t>> res( na, std::vector<uint32_t>( info.num_neurons ) );
+					std::vector<void *> ptrs;
+					for( auto & a : res ) ptrs.push_back( a.data() );
+					if( r == SPK_OK ) r = spk_net_neurons( j.net, ptrs.data() );
+					if( r != SPK_OK )
+					{
+						leaving[i].second = SPK_JOB_FAILED;
+						errs[i] = r;
+						emsgs[i] = spk_last_error();
+					}
+					else
+					{
+						j.result = std::move( res );
+						j.num_neurons = info.num_neurons;
+					}
+				}
+				spk_batch_remove( batch, j.net );
+				spk_net_destroy( j.net );
+				j.net = nullptr;
+			}
+			lk.lock();
+			for( size_t i = 0; i < leaving.size(); i++ )
+			{
+				job & j = *leaving[i].first;
+				in_use -= j.reserved;
+				j.reserved = 0;
+				finish( j, leaving[i].second, errs[i], emsgs[i] );
+			}
+		}
+	}
+};
+} // namespace
+
+struct spk_server : server
+{
+};
+
+extern "C" {
+int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps )
+{
+	if( !out ) return fail( SPK_ERR_INVALID, "out is null" );
+	*out = nullptr;
+	if( budget_bytes == 0 || quantum_steps == 0 ) return fail( SPK_ERR_INVALID, "budget and quantum must be > 0" );
+	auto s = std::make_unique<spk_server>();
+	s->device = device;
+	s->budget = budget_bytes;
+	s->quantum = quantum_steps;
+	if( cudaDeviceGetAttribute( &s->sms, cudaDevAttrMultiProcessorCount, device ) != cudaSuccess )
+		return fail( SPK_ERR_INVALID, "invalid device" );
+	int const rc = spk_batch_create( &s->batch, device );
+	if( rc != SPK_OK ) return rc;
+	s->worker = std::thread( [p = s.get()] { p->loop(); } );
+	*out = s.release();
+	return SPK_OK;
+}
+
+int spk_server_submit(
+    spk_server * s,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    uint64_t nsteps,
+    double timeout_s,
+    uint64_t * out_job )
+{
+	if( !s || !desc || !out_job ) return fail( SPK_ERR_INVALID, "null argument" );
+	if( nsteps == 0 ) return fail( SPK_ERR_INVALID, "nsteps must be > 0" );
+	if( model == SPK_BRUNEL_PLUS && delay > 63 ) return fail( SPK_ERR_INVALID, "plastic models support delays up to 63 steps" );
+	if( desc->npops <= 0 || !desc->pops || desc->nconn < 0 || ( desc->nconn && ( !desc->conn_src || !desc->conn_dst || !desc->conn_p ) ) )
+		return fail( SPK_ERR_INVALID, "bad layout descriptor" );
+	auto j = std::make_unique<job>();
+	j->model = model;
+	j->pops.assign( desc->pops, desc->pops + desc->npops );
+	j->src.assign( desc->conn_src, desc->conn_src + desc->nconn );
+	j->dst.assign( desc->conn_dst, desc->conn_dst + desc->nconn );
+	j->p.assign( desc->conn_p, desc->conn_p + desc->nconn );
+	j->dt = dt;
+	j->delay = delay;
+	j->seed = seed;
+	j->graph_seed = graph_seed;
+	j->nsteps = nsteps;
+	j->timeout_s = timeout_s;
+	// admission estimate at the largest tiling (one tile per SM), and the job's work share
+	uint64_t est = 0;
+	auto const d = j->desc();
+	int const rc = spk_net_estimate_bytes( model, &d, delay, s->device, 0, &est );
+	if( rc != SPK_OK ) return rc;
+	double syn = 0, n = 0;
+	for( int i = 0; i < desc->nconn; i++ )
+		syn += (double)desc->pops[desc->conn_src[i]] * (double)desc->pops[desc->conn_dst[i]] * desc->conn_p[i];
+	for( int i = 0; i < desc->npops; i++ ) n += (double)desc->pops[i];
+	j->work = syn * 0.01 + 1000.0 * n;
+	std::lock_guard<std::mutex> lk( s->mu );
+	j->id = s->next_id++;
+	j->t_submit = s->now();
+	j->reserved = est;
+	*out_job = j->id;
+	if( est > s->budget )
+	{
+		j->state = SPK_JOB_REFUSED;
+		j->error = SPK_ERR_NOMEM;
+		j->message = "the job's device memory exceeds the server's budget";
+		j->t_end = j->t_submit;
+		j->reserved = 0;
+		s->jobs[j->id] = std::move( j );
+		return fail( SPK_ERR_NOMEM, "the job's device memory (" + std::to_string( est ) + " B) exceeds the budget" );
+	}
+	s->queue.push_back( j.get() );
+	s->jobs[j->id] = std::move( j );
+	s->wake.notify_all();
+	return SPK_OK;
+}
+
+int spk_server_job_info( spk_server * s, uint64_t id, spk_job_info * out )
+{
+	if( !s || !out ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	auto it = s->jobs.find( id );
+	if( it == s->jobs.end() ) return fail( SPK_ERR_INVALID, "unknown job" );
+	job const & j = *it->second;
+	std::memset( out, 0, sizeof *out );
+	out->state = j.state;
+	out->error = j.error;
+	out->steps_done = j.done;
+	out->steps_total = j.nsteps;
+	out->num_neurons = j.num_neurons;
+	out->device_bytes = j.reserved;
+	out->t_submit = j.t_submit;
+	out->t_start = j.t_start;
+	out->t_end = j.t_end;
+	std::strncpy( out->message, j.message.c_str(), sizeof out->message - 1 );
+	return SPK_OK;
+}
+
+int spk_server_job_neurons( spk_server * s, uint64_t id, void * const * attrs )
+{
+	if( !s || !attrs ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	auto it = s->jobs.find( id );
+	if( it == s->jobs.end() ) return fail( SPK_ERR_INVALID, "unknown job" );
+	job const & j = *it->second;
+	if( j.state != SPK_JOB_DONE ) return fail( SPK_ERR_INVALID, "the job has not completed" );
+	for( size_t a = 0; a < j.result.size(); a++ )
+	{
+		if( !attrs[a] ) return fail( SPK_ERR_INVALID, "attribute pointer is null" );
+		std::memcpy( attrs[a], j.result[a].data(), j.result[a].size() * 4 );
+	}
+	return SPK_OK;
+}
+
+int spk_server_cancel( spk_server * s, uint64_t id )
+{
+	if( !s ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	auto it = s->jobs.find( id );
+	if( it == s->jobs.end() ) return fail( SPK_ERR_INVALID, "unknown job" );
+	it->second->cancel = true;
+	s->wake.notify_all();
+	return SPK_OK;
+}
+
+int spk_server_release( spk_server * s, uint64_t id )
+{
+	if( !s ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	auto it = s->jobs.find( id );
+	if( it == s->jobs.end() ) return fail( SPK_ERR_INVALID, "unknown job" );
+	if( !it->second->final() ) return fail( SPK_ERR_INVALID, "the job is still queued or running" );
+	s->jobs.erase( it );
+	return SPK_OK;
+}
+
+int spk_server_wait( spk_server * s, uint64_t id, double timeout_s )
+{
+	if( !s ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::unique_lock<std::mutex> lk( s->mu );
+	auto done = [&] {
+		if( id == 0 )
+		{
+			for( auto const & kv : s->jobs )
+				if( !kv.second->final() ) return false;
+			return true;
+		}
+		auto it = s->jobs.find( id );
+		return it == s->jobs.end() || it->second->final();
+	};
+	if( id != 0 && !s->jobs.count( id ) ) return fail( SPK_ERR_INVALID, "unknown job" );
+	if( timeout_s < 0 )
+		s->changed.wait( lk, done );
+	else if( !s->changed.wait_for( lk, std::chrono::duration<double>( timeout_s ), done ) )
+		return fail( SPK_ERR_TIMEOUT, "wait timed out" );
+	return SPK_OK;
+}
+
+int spk_server_get_stats( spk_server * s, spk_server_stats * out )
+{
+	if( !s || !out ) return fail( SPK_ERR_INVALID, "null argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	std::memset( out, 0, sizeof *out );
+	for( auto const & kv : s->jobs )
+		switch( kv.second->state )
+		{
+		case SPK_JOB_QUEUED: out->queued++; break;
+		case SPK_JOB_RUNNING: out->running++; break;
+		case SPK_JOB_DONE: out->done++; break;
+		case SPK_JOB_FAILED: out->failed++; break;
+		case SPK_JOB_CANCELLED: out->cancelled++; break;
+		case SPK_JOB_TIMEOUT: out->timed_out++; break;
+		case SPK_JOB_REFUSED: out->refused++; break;
+		}
+	out->bytes_in_use = s->in_use;
+	out->peak_bytes = s->peak;
+	out->budget_bytes = s->budget;
+	out->ticks = s->ticks;
+	return SPK_OK;
+}
+
+int spk_server_inject_alloc_failures( spk_server * s, int count )
+{
+	if( !s || count < 0 ) return fail( SPK_ERR_INVALID, "bad argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	s->inject = count;
+	return SPK_OK;
+}
+
+int spk_server_destroy( spk_server * s )
+{
+	if( !s ) return SPK_OK;
+	{
+		std::lock_guard<std::mutex> lk( s->mu );
+		s->stop = true;
+		s->wake.notify_all();
+	}
+	if( s->worker.joinable() ) s->worker.join();
+	for( auto * j : s->running )
+	{
+		spk_batch_remove( s->batch, j->net );
+		spk_net_destroy( j->net );
+		j->net = nullptr;
+	}
+	spk_batch_destroy( s->batch );
+	delete s;
+	return SPK_OK;
+}
+}

@@ -59,3 +59,16 @@ def test_layout_matches_reference_known_answers(lib):
     assert L(100, 1.0).max_degree() == 128
     assert L(100, 0.0).max_degree() == 0
     assert L([70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)]).max_degree() == 7328
+
+
+def test_server_and_batch_arguments_checked_without_device(lib):
+    import ctypes as C
+
+    h = C.c_void_p()
+    assert lib.spk_server_create(C.byref(h), 0, 0, 10) == spice_b200.ERR_INVALID  # zero budget
+    assert lib.spk_server_create(None, 0, 1 << 30, 10) == spice_b200.ERR_INVALID
+    assert lib.spk_server_wait(None, 0, 0.0) == spice_b200.ERR_INVALID
+    assert lib.spk_batch_run(None, 1) == spice_b200.ERR_INVALID
+    assert lib.spk_batch_add(None, None) == spice_b200.ERR_INVALID
+    assert lib.spk_server_destroy(None) == spice_b200.OK
+    assert lib.spk_batch_destroy(None) == spice_b200.OK
