@@ -458,16 +458,22 @@ def run_serving(args, rank, world):
     clocks = Clocks(dev)
     clocks.start()
     # (a) plain loop, real time
-    lat_plain = []
+    lat_plain, build_plain = [], 0.0
+    run_plain = {m: 0.0 for m in BATCH_MODELS}
     t0 = time.perf_counter()
     for j in jobs:
         now = time.perf_counter() - t0
         if now < j["t"]:
             time.sleep(j["t"] - now)
+        tb = time.perf_counter()
         net = Snn(j["model"], Layout(j["pops"], j["conns"]), dt=DT, delay=j["delay"], seed=j["seed"],
                   graph_seed=1000 + j["seed"], device=dev)
+        net.sync()
+        tr = time.perf_counter()
+        build_plain += tr - tb
         net.run(j["steps"])
         net.sync()
+        run_plain[j["model"]] += time.perf_counter() - tr
         net.close()
         lat_plain.append(time.perf_counter() - t0 - j["t"])
     span_plain = time.perf_counter() - t0
@@ -500,9 +506,10 @@ def run_serving(args, rank, world):
                            "syn_range": [1e6, 2e8], "bio_range_s": [0.1, 2.0], "arrival_s": args.duration,
                            "budget_gb": args.budget_gb, "quantum_steps": args.quantum},
                 "server": {"p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "span_s": span, "done": states.count(2),
-                           "peak_gb": st["peak_bytes"] / 1e9, "ticks": st["ticks"]},
+                           "peak_gb": st["peak_bytes"] / 1e9, "ticks": st["ticks"],
+                           "build_s": st["build_seconds"], "tick_s": st["tick_seconds"]},
                 "plain_loop": {"p50_s": pct(lat_plain, 50), "p99_s": pct(lat_plain, 99), "span_s": span_plain,
-                               "value": work / span_plain},
+                               "value": work / span_plain, "build_s": build_plain, "run_s_by_model": run_plain},
                 "speedup_vs_plain_loop": span_plain / span, "clocks": clk}
         print(json.dumps(line), flush=True)
 

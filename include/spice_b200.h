@@ -222,7 +222,8 @@ int spk_batch_run_nets( spk_batch * batch, int count, spk_net * const * nets, ui
 int spk_batch_destroy( spk_batch * batch );
 
 /* ---- serving: jobs admitted against a device-memory budget, continuously batched ----
- * A server owns one worker thread and one batch on `device`. Submitted jobs queue in
+ * A server owns two worker threads (one builds admitted jobs' nets, one steps the batch)
+ * and one batch on `device`. Submitted jobs queue in
  * arrival order; the head is admitted when its estimated device memory
  * (spk_net_estimate_bytes) fits the budget beside the running jobs, and its net is built
  * with a tile count sized to its share of the load. Every tick advances each running job
@@ -261,6 +262,8 @@ typedef struct spk_server_stats
 	uint64_t queued, running, done, failed, cancelled, timed_out, refused;
 	uint64_t bytes_in_use, peak_bytes, budget_bytes;
 	uint64_t ticks;
+	double build_seconds; /* building admitted jobs' nets (builder thread)          */
+	double tick_seconds;  /* ticks: batch runs until every stepped net synchronised */
 } spk_server_stats;
 
 int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps );
@@ -291,7 +294,7 @@ int spk_server_get_stats( spk_server * server, spk_server_stats * out );
 /* Fault injection on the host: the next `count` admissions fail as an allocation failure
  * would (the job ends FAILED with SPK_ERR_NOMEM; the server carries on). */
 int spk_server_inject_alloc_failures( spk_server * server, int count );
-/* Stops the worker; running jobs are dropped. */
+/* Stops both threads; queued and running jobs are dropped. */
 int spk_server_destroy( spk_server * server );
 
 #ifdef __cplusplus

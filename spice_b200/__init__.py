@@ -85,7 +85,8 @@ class JobInfo(C.Structure):  # spk_job_info
 
 class ServerStats(C.Structure):  # spk_server_stats
     _fields_ = [(k, C.c_uint64) for k in ("queued", "running", "done", "failed", "cancelled", "timed_out", "refused",
-                                          "bytes_in_use", "peak_bytes", "budget_bytes", "ticks")]
+                                          "bytes_in_use", "peak_bytes", "budget_bytes", "ticks")] + [
+        ("build_seconds", C.c_double), ("tick_seconds", C.c_double)]
 
 
 JOB_STATES = ("queued", "running", "done", "failed", "cancelled", "timeout", "refused")
@@ -423,7 +424,7 @@ def estimate_bytes(model, layout, delay=1, device=0, tile_target=0):
 
 class Server:
     """Simulation jobs admitted against a device-memory budget and stepped by continuous
-    batching on one GPU (a native worker thread; see spk_server_* in spice_b200.h).
+    batching on one GPU (native builder and ticker threads; see spk_server_* in spice_b200.h).
 
     srv = Server(budget_bytes=150e9, quantum=1500)
     job = srv.submit("brunel", layout, nsteps=10_000, delay=15, seed=1)

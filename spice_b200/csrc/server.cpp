@@ -2,15 +2,16 @@
 // budget, stepped together by continuous batching.
 //
 // The reference has no server; a workload of many nets is a host loop that builds and steps
-// one net after another (spice_bench/paper_plots.cpp:184-231). Here one worker thread per
-// server owns the GPU side:
-//   admit   queued jobs in arrival order while their estimated device memory fits the
-//           budget (a job larger than the whole budget is refused at submission); each
-//           admitted job's net is built with a tile count sized to its share of the load;
-//   tick    every running job advances by up to `quantum` steps in one batch run (jobs
-//           admitted since the last tick join it: continuous batching);
-//   retire  finished jobs export their final neuron state to host memory and free their
-//           device memory; cancelled, timed-out and failed jobs free theirs too.
+// one net after another (spice_bench/paper_plots.cpp:184-231). Here two threads per server
+// own the GPU side:
+//   builder  admits queued jobs in arrival order while their estimated device memory fits
+//            the budget (a job larger than the whole budget is refused at submission) and
+//            builds each admitted job's net, with a tile count sized to its share of the
+//            load, while the ticker steps the others;
+//   ticker   each tick advances every running job by up to `quantum` steps in one batch
+//            run (jobs built since the last tick join it: continuous batching), then
+//            retires: finished jobs export their final neuron state to host memory and free
+//            their device memory; cancelled, timed-out and failed jobs free theirs too.
 // The server is a client of the C ABI only (spk_net_*, spk_batch_*): a job's results are
 // those of the same net stepped alone.
 #include <spice_b200.h>
@@ -86,10 +87,14 @@ struct server
 	uint64_t next_id = 1;
 	std::map<uint64_t, std::unique_ptr<job>> jobs;
 	std::deque<job *> queue;
-	std::vector<job *> running;
+	std::vector<job *> building, ready; // admitted: net being built / built, not yet ticked
+	std::vector<job *> running;         // in the batch (copy of the ticker's list)
+	std::vector<job *> running_t;       // the ticker's own list
+	std::condition_variable tick_wake;
 	uint64_t in_use = 0, peak = 0, ticks = 0;
+	double build_s = 0, tick_s = 0;
 	int inject = 0;
-	std::thread worker;
+	std::thread builder, ticker;
 
 	double now() const { return std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count(); }
 
@@ -111,28 +116,27 @@ struct server
 		return std::max( 1, (int)std::lround( sms * j.work / total ) );
 	}
 
-	// build the net of an admitted job (lock not held)
+	// build the net of an admitted job (lock not held; the ticker adds it to the batch)
 	int build( job & j, int target, std::string & msg )
 	{
 		auto const d = j.desc();
-		int rc = spk_net_create_ex( &j.net, j.model, &d, j.dt, j.delay, j.seed, j.graph_seed, device, target );
-		if( rc == SPK_OK ) rc = spk_batch_add( batch, j.net );
+		int const rc = spk_net_create_ex( &j.net, j.model, &d, j.dt, j.delay, j.seed, j.graph_seed, device, target );
 		if( rc != SPK_OK )
 		{
 			msg = spk_last_error();
-			if( j.net ) spk_net_destroy( j.net );
 			j.net = nullptr;
 		}
 		return rc;
 	}
 
-	void loop()
+	// builder thread: deadlines of queued jobs, admission in arrival order while the head
+	// fits the budget, and the admitted jobs' nets (built while the ticker steps others)
+	void build_loop()
 	{
 		std::unique_lock<std::mutex> lk( mu );
 		while( !stop )
 		{
 			double const t = now();
-			// queued jobs: cancellations and deadlines
 			for( auto it = queue.begin(); it != queue.end(); )
 			{
 				job & j = **it;
@@ -144,41 +148,79 @@ struct server
 				else
 					++it;
 			}
-			// admission in arrival order while the head fits the budget
-			while( !queue.empty() && in_use + queue.front()->reserved <= budget && !stop )
-			{
-				job & j = *queue.front();
-				queue.pop_front();
-				in_use += j.reserved;
-				peak = std::max( peak, in_use );
-				j.state = SPK_JOB_RUNNING;
-				j.t_start = now();
-				int const target = tile_target( j );
-				bool const injected = inject > 0;
-				if( injected ) inject--;
-				lk.unlock();
-				std::string msg;
-				int const rc = injected ? ( msg = "injected allocation failure", SPK_ERR_NOMEM ) : build( j, target, msg );
-				lk.lock();
-				if( rc != SPK_OK )
-				{
-					in_use -= j.reserved;
-					j.reserved = 0;
-					finish( j, SPK_JOB_FAILED, rc, msg );
-					continue;
-				}
-				running.push_back( &j );
-			}
-			if( running.empty() )
+			if( queue.empty() || in_use + queue.front()->reserved > budget )
 			{
 				wake.wait_for( lk, std::chrono::milliseconds( 20 ) );
+				continue;
+			}
+			job & j = *queue.front();
+			queue.pop_front();
+			in_use += j.reserved;
+			peak = std::max( peak, in_use );
+			j.state = SPK_JOB_RUNNING;
+			j.t_start = now();
+			int const target = tile_target( j );
+			bool const injected = inject > 0;
+			if( injected ) inject--;
+			building.push_back( &j );
+			lk.unlock();
+			std::string msg;
+			double const tb = now();
+			int const rc = injected ? ( msg = "injected allocation failure", SPK_ERR_NOMEM ) : build( j, target, msg );
+			lk.lock();
+			build_s += now() - tb;
+			building.erase( std::find( building.begin(), building.end(), &j ) );
+			if( rc != SPK_OK )
+			{
+				in_use -= j.reserved;
+				j.reserved = 0;
+				finish( j, SPK_JOB_FAILED, rc, msg );
+				continue;
+			}
+			ready.push_back( &j );
+			tick_wake.notify_all();
+		}
+	}
+
+	// ticker thread: built jobs join the batch; every tick advances each running job by up
+	// to `quantum` steps; finished, failed, cancelled and timed-out jobs leave
+	void tick_loop()
+	{
+		std::unique_lock<std::mutex> lk( mu );
+		while( !stop )
+		{
+			std::vector<job *> joining;
+			joining.swap( ready );
+			lk.unlock();
+			std::vector<std::pair<job *, std::string>> rejected;
+			for( auto * j : joining )
+				if( spk_batch_add( batch, j->net ) == SPK_OK )
+					running_t.push_back( j );
+				else
+					rejected.push_back( { j, spk_last_error() } );
+			for( auto & r : rejected )
+			{
+				spk_net_destroy( r.first->net );
+				r.first->net = nullptr;
+			}
+			lk.lock();
+			for( auto & r : rejected )
+			{
+				in_use -= r.first->reserved;
+				r.first->reserved = 0;
+				finish( *r.first, SPK_JOB_FAILED, SPK_ERR_INVALID, r.second );
+			}
+			running = running_t;
+			if( running_t.empty() )
+			{
+				tick_wake.wait_for( lk, std::chrono::milliseconds( 20 ) );
 				continue;
 			}
 			// one tick: every running job up to `quantum` steps
 			std::vector<spk_net *> nets;
 			std::vector<uint64_t> counts;
 			std::vector<job *> ticked;
-			for( auto * j : running )
+			for( auto * j : running_t )
 				if( !j->cancel && j->done < j->nsteps )
 				{
 					nets.push_back( j->net );
@@ -186,6 +228,7 @@ struct server
 					ticked.push_back( j );
 				}
 			lk.unlock();
+			double const tt = now();
 			std::vector<int> status( ticked.size(), SPK_OK );
 			std::vector<std::string> msgs( ticked.size() );
 			int rc = nets.empty() ? SPK_OK : spk_batch_run_nets( batch, (int)nets.size(), nets.data(), counts.data() );
@@ -197,14 +240,15 @@ struct server
 			}
 			lk.lock();
 			ticks++;
+			tick_s += now() - tt;
 			for( size_t i = 0; i < ticked.size(); i++ )
 				if( status[i] == SPK_OK ) ticked[i]->done += counts[i];
-			// retire: finished, failed, cancelled and timed-out jobs
+			// retire
 			double const te = now();
 			std::vector<std::pair<job *, int>> leaving; // (job, final state)
 			std::vector<int> errs;
 			std::vector<std::string> emsgs;
-			for( auto it = running.begin(); it != running.end(); )
+			for( auto it = running_t.begin(); it != running_t.end(); )
 			{
 				job & j = **it;
 				auto const k = std::find( ticked.begin(), ticked.end(), &j ) - ticked.begin();
@@ -222,8 +266,9 @@ struct server
 				leaving.push_back( { &j, state } );
 				errs.push_back( st );
 				emsgs.push_back( (size_t)k < ticked.size() ? msgs[k] : std::string() );
-				it = running.erase( it );
+				it = running_t.erase( it );
 			}
+			running = running_t;
 			lk.unlock();
 			for( size_t i = 0; i < leaving.size(); i++ )
 			{
@@ -263,6 +308,7 @@ struct server
 				j.reserved = 0;
 				finish( j, leaving[i].second, errs[i], emsgs[i] );
 			}
+			if( !leaving.empty() ) wake.notify_all(); // budget freed
 		}
 	}
 };
@@ -286,7 +332,8 @@ int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uin
 		return fail( SPK_ERR_INVALID, "invalid device" );
 	int const rc = spk_batch_create( &s->batch, device );
 	if( rc != SPK_OK ) return rc;
-	s->worker = std::thread( [p = s.get()] { p->loop(); } );
+	s->builder = std::thread( [p = s.get()] { p->build_loop(); } );
+	s->ticker = std::thread( [p = s.get()] { p->tick_loop(); } );
 	*out = s.release();
 	return SPK_OK;
 }
@@ -452,6 +499,8 @@ int spk_server_get_stats( spk_server * s, spk_server_stats * out )
 	out->peak_bytes = s->peak;
 	out->budget_bytes = s->budget;
 	out->ticks = s->ticks;
+	out->build_seconds = s->build_s;
+	out->tick_seconds = s->tick_s;
 	return SPK_OK;
 }
 
@@ -470,9 +519,13 @@ int spk_server_destroy( spk_server * s )
 		std::lock_guard<std::mutex> lk( s->mu );
 		s->stop = true;
 		s->wake.notify_all();
+		s->tick_wake.notify_all();
 	}
-	if( s->worker.joinable() ) s->worker.join();
-	for( auto * j : s->running )
+	if( s->builder.joinable() ) s->builder.join();
+	if( s->ticker.joinable() ) s->ticker.join();
+	for( auto * j : s->ready )
+		spk_net_destroy( j->net );
+	for( auto * j : s->running_t )
 	{
 		spk_batch_remove( s->batch, j->net );
 		spk_net_destroy( j->net );
