@@ -138,11 +138,13 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per launch of the window kernel from the committed ncu summary, if any."""
+    """DRAM bytes per simulated step of the window kernel from the committed ncu summary
+    (bytes per captured launch / steps per captured launch), if any."""
     path = os.path.join(ROOT, "profiles", "window_flat_brunel_1e9.json")
     try:
         with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_launch_full_size"])
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch_full_size"]) / float(d["steps_per_launch"])
     except Exception:
         return None
 
@@ -225,7 +227,6 @@ def run_ours(args, rank, world):
     info = net.info()
     stream = torch.cuda.ExternalStream(net.stream(), device=dev)
     S = args.sim_steps
-    windows_per_step = -(-S // DELAY)
 
     for _ in range(args.warmup):
         net.run(S)
@@ -237,6 +238,7 @@ def run_ours(args, rank, world):
 
     barrier(world)
     torch.cuda.synchronize()
+    launches0 = net.info().kernel_launches
     clocks = Clocks(dev)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -247,6 +249,8 @@ def run_ours(args, rank, world):
     ev1.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    launches = net.info().kernel_launches - launches0
+    persistent = bool(net.info().persistent)
     barrier(world)
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms, world)
@@ -272,12 +276,13 @@ def run_ours(args, rank, world):
     state_bytes = 8  # V, Twait
     bytes_per_step = (spikes_per_step * mean_degree * 4 + spikes_per_step * info.num_tiles * 4 + 4 * n * state_bytes
                       + spikes_per_step * 4)
-    bytes_per_window = DELAY * bytes_per_step
-    launches = args.steps * windows_per_step
+    steps_per_launch = args.steps * S / launches
+    bytes_per_launch = steps_per_launch * bytes_per_step
     t_launch = (ms / 1e3) / launches
     peak, peak_kind = measured_peaks()
-    achieved = bytes_per_window / t_launch / 1e9
-    traffic = profile_traffic()
+    achieved = bytes_per_launch / t_launch / 1e9
+    traffic_per_step = profile_traffic()
+    traffic = traffic_per_step * steps_per_launch if traffic_per_step else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
@@ -289,7 +294,9 @@ def run_ours(args, rank, world):
                            "spikes_per_step": spikes_per_step},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "traffic": traffic, "peak_kind": peak_kind, "kernel": "window_flat<brunel>",
-                             "bytes_per_launch": bytes_per_window, "launch_us": t_launch * 1e6},
+                             "bytes_per_launch": bytes_per_launch, "launch_us": t_launch * 1e6,
+                             "steps_per_launch": steps_per_launch, "persistent": persistent,
+                             "bytes_per_step": bytes_per_step},
                 "e2e": {"value": e2e_wall / (S * DT * world), "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": int(statistics.median(d2h))},
                 "gpu_launches": launches, "clocks": clk}

@@ -63,6 +63,9 @@ typedef struct spk_net_info
 	uint64_t tile_size;    /* destination neurons per tile (one CTA each)                */
 	uint64_t num_tiles;
 	uint64_t device_bytes; /* device memory held by the net                              */
+	uint64_t kernel_launches; /* simulation kernel launches so far (a CUDA graph's replay
+	                             counts each window; a batch counts its shared launches)  */
+	int persistent;        /* 1: spk_net_run advances the net in one cooperative launch */
 } spk_net_info;
 
 /* Message of the last failed call on this host thread ("" if none). */

@@ -65,6 +65,8 @@ class NetInfo(C.Structure):
         ("tile_size", C.c_uint64),
         ("num_tiles", C.c_uint64),
         ("device_bytes", C.c_uint64),
+        ("kernel_launches", C.c_uint64),
+        ("persistent", C.c_int),
     ]
 
 

@@ -475,9 +475,23 @@ __global__ void init_neurons( net_params p )
 	}
 }
 
-// Dense, ascending copy of the spikes of `count` consecutive steps starting at step t0
-// from the ring into out_ids; out_counts[k] = spikes of step t0 + k; *cursor advances by
-// the total. One CTA per step; the last CTA to finish moves the cursor.
+// spikes per step of the `count` steps just simulated (the clock already advanced past
+// them): totals[k] = sum over tiles of the step's ring counts; one warp per step
+__global__ void raster_totals( unsigned const * ring_cnt, int ntiles, int ring, clock_state const * clock, int count, unsigned * totals )
+{
+	int const k = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5, lane = threadIdx.x & 31;
+	if( k >= count ) return;
+	long long const t0 = clock->step - count;
+	int const slot = (int)( ( t0 + k ) % ring );
+	unsigned c = 0;
+	for( int i = lane; i < ntiles; i += 32 ) c += ring_cnt[(long long)slot * ntiles + i];
+	for( int o = 16; o > 0; o >>= 1 ) c += __shfl_xor_sync( ~0u, c, o );
+	if( lane == 0 ) totals[k] = c;
+}
+
+// Dense raster of the `count` steps just simulated: step k's spikes (ascending: tiles in
+// order, each tile's ids ascending) go to out_ids at cursor + (spikes of steps < k); the
+// last block advances the cursor. totals = raster_totals of the same steps.
 __global__ void gather_raster(
     int const * ring_ids,
     unsigned const * ring_cnt,
@@ -487,38 +501,49 @@ __global__ void gather_raster(
     int ring,
     clock_state const * clock,
     int count,
+    unsigned const * totals,
     unsigned long long * cursor,
     unsigned * done,
     int * out_ids,
-    unsigned * out_counts,
     unsigned long long out_cap,
     int * err )
 {
 	__shared__ int scratch[33];
 	__shared__ long long s_base;
-	__shared__ int s_off;
+	__shared__ long long s_off, s_grand;
 	int const k = blockIdx.x, tid = threadIdx.x;
-	// the window that produced these steps already advanced the clock
 	long long const t0 = clock->step - count;
-	// offset of step k inside this batch = sum of the totals of the steps before it;
-	// grand = total of the whole batch
-	int before = 0, grand = 0;
-	for( int s = 0; s < count; s++ )
+	// offset of step k = spikes of the steps before it; grand = all of them
+	long long before = 0, grand = 0;
+	for( int s = tid; s < count; s += blockDim.x )
 	{
-		int const slot = (int)( ( t0 + s ) % ring );
-		for( int base = 0; base < ntiles; base += blockDim.x )
-		{
-			int const i = base + tid;
-			int tot;
-			block_exclusive_scan( i < ntiles ? (int)ring_cnt[(long long)slot * ntiles + i] : 0, scratch, &tot );
-			if( s < k ) before += tot;
-			grand += tot;
-		}
+		long long const c = totals[s];
+		grand += c;
+		if( s < k ) before += c;
 	}
+	for( int o = 16; o > 0; o >>= 1 )
+	{
+		before += __shfl_xor_sync( ~0u, before, o );
+		grand += __shfl_xor_sync( ~0u, grand, o );
+	}
+	__shared__ long long s_red[2][32];
+	if( ( tid & 31 ) == 0 )
+	{
+		s_red[0][tid >> 5] = before;
+		s_red[1][tid >> 5] = grand;
+	}
+	__syncthreads();
 	if( tid == 0 )
 	{
+		long long b = 0, g = 0;
+		for( int w = 0; w < (int)( blockDim.x >> 5 ); w++ )
+		{
+			b += s_red[0][w];
+			g += s_red[1][w];
+		}
 		s_base = (long long)*cursor;
-		s_off = before;
+		s_off = b;
+		s_grand = g;
 	}
 	__syncthreads();
 	int const slot = (int)( ( t0 + k ) % ring );
@@ -541,15 +566,15 @@ __global__ void gather_raster(
 	}
 	if( tid == 0 )
 	{
-		if( out_counts ) out_counts[k] = (unsigned)running;
 		__threadfence();
 		unsigned const prev = atomicAdd( done, 1u );
 		if( prev == gridDim.x - 1 )
 		{
-			*cursor = (unsigned long long)( s_base + grand );
+			*cursor = (unsigned long long)( s_base + s_grand );
 			*done = 0;
 			__threadfence();
 		}
 	}
 }
+
 } // namespace spk

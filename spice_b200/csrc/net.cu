@@ -226,6 +226,8 @@ struct spk_net
 
 	unsigned long long steps = 0;   // steps requested so far
 	unsigned long long launched = 0; // steps launched
+	unsigned long long kernel_launches = 0; // simulation kernel launches (graph replays counted per window)
+	int ring_slots = 0;                      // steps the spike ring holds (2 delay; more for recording runs)
 	unsigned * host_count = nullptr; // pinned
 
 	cudaGraphExec_t graph = nullptr;
@@ -258,7 +260,7 @@ struct spk_net
 		p.delay = delay;
 		p.tile = tc.tile;
 		p.ntiles = tc.ntiles;
-		p.ring = 2 * delay;
+		p.ring = ring_slots;
 		p.seed = seed;
 		p.edges = edges.as<int const>();
 		p.pivots = pivots.as<unsigned const>();
@@ -417,6 +419,7 @@ struct spk_net
 			int const L = (int)std::min<unsigned long long>( steps - launched, (unsigned long long)max_window() );
 			launch_window( L );
 			launched += L;
+			kernel_launches++;
 		}
 	}
 
@@ -437,22 +440,55 @@ struct spk_net
 	// dense ascending spikes of the `count` steps just launched -> ids (device), counts
 	void gather( int count, int * ids, unsigned * counts, unsigned long long cap, long long rec_base )
 	{
+		spk::raster_totals<<<( count + 7 ) / 8, 256, 0, stream>>>(
+		    ring_cnt.as<unsigned>(), tc.ntiles, ring_slots, clock.as<spk::clock_state>(), count, counts + rec_base );
+		CK( cudaGetLastError() );
 		spk::gather_raster<<<count, 256, 0, stream>>>(
 		    ring_ids.as<int>(),
 		    ring_cnt.as<unsigned>(),
 		    (int)n,
 		    tile_first.as<int>(),
 		    tc.ntiles,
-		    2 * delay,
+		    ring_slots,
 		    clock.as<spk::clock_state>(),
 		    count,
+		    counts + rec_base,
 		    cursor.as<unsigned long long>(),
 		    gather_done.as<unsigned>(),
 		    ids,
-		    counts ? counts + rec_base : nullptr,
 		    cap,
 		    err.as<int>() );
 		CK( cudaGetLastError() );
+	}
+
+	// Enlarge the spike ring to `slots` steps (window_flat nets, all steps launched): the
+	// last ring_slots steps' spikes move to their slots of the larger ring, so a
+	// persistent run of up to slots - 2 delay steps leaves every step it simulated in
+	// the ring for one gather at the end.
+	void grow_ring( int slots )
+	{
+		if( slots <= ring_slots ) return;
+		require( flat && model != SPK_BRUNEL_PLUS && launched == steps, "ring growth of a window_flat net between runs" );
+		dbuf ids, cnt;
+		ids.alloc( (size_t)slots * n * 4 );
+		cnt.alloc( (size_t)slots * tc.ntiles * 4 );
+		CK( cudaMemsetAsync( cnt.p, 0, cnt.bytes, stream ) );
+		long long const t = (long long)launched;
+		for( long long st = std::max( 0LL, t - ring_slots ); st < t; st++ )
+		{
+			long long const from = st % ring_slots, to = st % slots;
+			CK( cudaMemcpyAsync( ids.as<int>() + to * n, ring_ids.as<int>() + from * n, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream ) );
+			CK( cudaMemcpyAsync( cnt.as<unsigned>() + to * tc.ntiles, ring_cnt.as<unsigned>() + from * tc.ntiles, (size_t)tc.ntiles * 4,
+			                     cudaMemcpyDeviceToDevice, stream ) );
+		}
+		CK( cudaStreamSynchronize( stream ) );
+		std::swap( ring_ids.p, ids.p );
+		std::swap( ring_ids.bytes, ids.bytes );
+		std::swap( ring_cnt.p, cnt.p );
+		std::swap( ring_cnt.bytes, cnt.bytes );
+		ring_slots = slots;
+		if( graph ) cudaGraphExecDestroy( graph ); // captured the old ring
+		graph = nullptr;
 	}
 
 	void build_graph_exec( int windows, int len )
@@ -506,6 +542,7 @@ struct spk_net
 				int const L = (int)std::min<unsigned long long>( nsteps, 1u << 30 );
 				steps += L;
 				launch_persistent( L );
+				kernel_launches++;
 				launched += L;
 				nsteps -= L;
 			}
@@ -520,6 +557,7 @@ struct spk_net
 			while( nsteps >= per_graph )
 			{
 				CK( cudaGraphLaunch( graph, stream ) );
+				kernel_launches += windows;
 				nsteps -= per_graph;
 				steps += per_graph;
 				launched += per_graph;
@@ -753,8 +791,9 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.edges.alloc( (size_t)( n * width ) * 4 );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
-	net.ring_ids.alloc( (size_t)2 * net.delay * n * 4 );
-	net.ring_cnt.alloc( (size_t)2 * net.delay * net.tc.ntiles * 4 );
+	net.ring_slots = 2 * net.delay;
+	net.ring_ids.alloc( (size_t)net.ring_slots * n * 4 );
+	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4 );
 	net.clock.alloc( sizeof( spk::clock_state ) );
 	net.dt_ring.alloc( spk::DT_RING * 4 );
 	net.err.alloc( 4 );
@@ -842,6 +881,9 @@ void enqueue_pivots( spk_net & net )
 	if( net.flat ) build_slices( net );
 }
 
+// device memory a recording run may give the spike ring (run_record of persistent nets)
+constexpr long long RECORD_RING_BYTES = 1LL << 30;
+
 // Re-tile a net that has not been stepped yet for about `target` tiles (batching): tiles,
 // pivots, slices and the per-tile buffers are rebuilt from the unchanged edges.
 void retile( spk_net & net, int target )
@@ -853,7 +895,7 @@ void retile( spk_net & net, int target )
 	CK( cudaStreamSynchronize( net.stream ) );
 	require( flat_tiling( net, segs, target ), "tiling failed" );
 	net.pivots.alloc( (size_t)net.n * ( net.tc.ntiles + 1 ) * 4 );
-	net.ring_cnt.alloc( (size_t)2 * net.delay * net.tc.ntiles * 4 );
+	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4 );
 	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
 	enqueue_pivots( net );
 	if( net.graph ) cudaGraphExecDestroy( net.graph );
@@ -1073,6 +1115,7 @@ struct spk_batch
 		{
 			gn[i]->steps += counts[i];
 			gn[i]->launched += counts[i];
+			gn[i]->kernel_launches += ( counts[i] + gn[i]->max_window() - 1 ) / gn[i]->max_window(); // shared launches
 		}
 		CK( cudaEventRecord( g.ev, g.stream ) );
 		for( auto * net : gn ) CK( cudaStreamWaitEvent( net->stream, g.ev, 0 ) );
@@ -1318,13 +1361,26 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 		if( net->rec_ids.bytes < std::max<uint64_t>( ids_cap, 1 ) * 4 ) net->rec_ids.alloc( std::max<uint64_t>( ids_cap, 1 ) * 4 );
 		if( net->rec_cnt.bytes < nsteps * 4 ) net->rec_cnt.alloc( nsteps * 4 );
 		CK( cudaMemsetAsync( net->cursor.p, 0, 8, net->stream ) );
+		// persistent nets record in chunks: one launch per chunk into a ring enlarged to
+		// hold the chunk (bounded to RECORD_RING_BYTES), one gather per chunk
+		long long chunk = 0;
+		if( net->persistent )
+		{
+			long long const per_slot = net->n * 4 + (long long)net->tc.ntiles * 4;
+			long long const fit = RECORD_RING_BYTES / per_slot - 2LL * net->delay;
+			chunk = std::min<long long>( { (long long)nsteps, fit, 1LL << 20 } );
+			if( chunk < 4LL * net->max_window() ) chunk = 0;
+			else net->grow_ring( (int)( chunk + 2 * net->delay ) );
+		}
 		uint64_t done = 0;
 		while( done < nsteps )
 		{
-			int const L = (int)std::min<uint64_t>( nsteps - done, (uint64_t)net->max_window() );
+			int const L = (int)std::min<uint64_t>( nsteps - done, chunk > 0 ? (uint64_t)chunk : (uint64_t)net->max_window() );
 			net->steps += L;
-			net->launch_window( L );
+			if( chunk > 0 ) net->launch_persistent( L );
+			else net->launch_window( L );
 			net->launched += L;
+			net->kernel_launches++;
 			net->gather( L, net->rec_ids.as<int>(), net->rec_cnt.as<unsigned>(), ids_cap, (long long)done );
 			done += L;
 		}
@@ -1381,6 +1437,8 @@ int spk_net_get_info( spk_net * net, spk_net_info * out )
 		out->tile_size = (uint64_t)net->tc.tile;
 		out->num_tiles = (uint64_t)net->tc.ntiles;
 		out->device_bytes = net->device_bytes();
+		out->kernel_launches = net->kernel_launches;
+		out->persistent = net->persistent ? 1 : 0;
 	} );
 }
 

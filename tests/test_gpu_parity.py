@@ -386,3 +386,32 @@ def test_nets_of_one_model_with_different_shared_memory(model, kernel, monkeypat
     small.run(30)
     big.sync()
     small.sync()
+
+
+@pytest.mark.parametrize("n,delay,chunks", [
+    (20_000, 15, [1050, 1050, 7, 300]),   # chunks of a persistent run, one gather each
+    (300_000, 6, [100, 2000, 5]),         # ring enlarged after steps were taken
+])
+def test_recording_runs_equal_windowed_recording(n, delay, chunks):
+    """run_record of a persistent net (one cooperative launch per chunk into an enlarged
+    spike ring) against run_record over windows; runs and stepped output after it agree."""
+    layout = Layout([n // 2, n // 2], [(0, 1, 16 / n), (1, 1, 16 / n)])
+    a = Snn("synth" if delay == 6 else "brunel", layout, delay=delay, seed=8, graph_seed=8)
+    os.environ["SPK_PERSIST"] = "0"
+    try:
+        b = Snn("synth" if delay == 6 else "brunel", layout, delay=delay, seed=8, graph_seed=8)
+    finally:
+        del os.environ["SPK_PERSIST"]
+    assert a.info().persistent == 1 and b.info().persistent == 0
+    a.run(37)
+    b.run(37)
+    for c in chunks:
+        ca, ia = a.run_record(c, cap=n * c // 4)
+        cb, ib = b.run_record(c, cap=n * c // 4)
+        assert np.array_equal(ca, cb) and np.array_equal(ia, ib), c
+    a.run(500)
+    b.run(500)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+    for k in range(2 * delay):
+        assert np.array_equal(a.step(out=True), b.step(out=True)), k
