@@ -66,6 +66,8 @@ typedef struct spk_net_info
 	uint64_t kernel_launches; /* simulation kernel launches so far (a CUDA graph's replay
 	                             counts each window; a batch counts its shared launches)  */
 	int persistent;        /* 1: spk_net_run advances the net in one cooperative launch */
+	int slice_pack;        /* window_flat slices: 8 (16-bit) or 12 (10-bit) indices per
+	                          16-byte vector; 0 for the other window kernels            */
 } spk_net_info;
 
 /* Message of the last failed call on this host thread ("" if none). */

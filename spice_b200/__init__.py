@@ -67,6 +67,7 @@ class NetInfo(C.Structure):
         ("device_bytes", C.c_uint64),
         ("kernel_launches", C.c_uint64),
         ("persistent", C.c_int),
+        ("slice_pack", C.c_int),
     ]
 
 

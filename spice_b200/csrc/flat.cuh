@@ -4,8 +4,9 @@
 // a CTA owns one tile of destination neurons [tile_first[j], tile_first[j + 1]).
 //
 // Data layout ("slices"). Besides the ELL rows, the net keeps every row's part inside
-// every tile as a slice of 16-bit counter indices, class(src) * span + (target - d0),
-// padded with SLICE_PAD to a whole 16-byte vector. A tile's slices lie contiguously in
+// every tile as a slice of counter indices, class(src) * span + (target - d0), padded to a
+// whole 16-byte vector: eight 16-bit indices per vector (pad SLICE_PAD), or, when every
+// index of the net fits 10 bits, twelve (three per 32-bit word, pad SLICE_PAD10). A tile's slices lie contiguously in
 // ascending source order, and rec[src * ntiles + tile] = { first vector, length }. So a
 // CTA reads only its own tile's region, two bytes per synapse, already in the form its
 // counters are indexed by.
@@ -53,6 +54,7 @@ constexpr int FLAT_MAX_TILE = 4064;   // slice lengths fit the table's 12-bit fi
 constexpr int FLAT_MIN_BUF = 512;     // vectors per buffer at least (one slice of a full tile)
 constexpr int FLAT_P_BITS = 20;       // vector offsets inside a step held in the table
 constexpr unsigned short SLICE_PAD = 0xFFFFu;
+constexpr unsigned SLICE_PAD10 = 0x3FFu; // 10-bit packing: indices < SLICE_PAD10
 static_assert( FLAT_SCRATCH >= FLAT_THREADS, "staging keeps one prefix per thread in the scratch" );
 static_assert( FLAT_STEP_CAP <= ( 1 << FLAT_P_BITS ), "step offsets fit the table" );
 
@@ -78,8 +80,11 @@ inline size_t flat_smem_bytes( int classes, int attrs, int tmax )
 // ------------------------------------------------------------------------------------
 // building the slices (once per net)
 // ------------------------------------------------------------------------------------
+// 16-byte vectors of a slice of `len` indices, `per` (8 or 12) to a vector
+__host__ __device__ __forceinline__ unsigned slice_vecs( unsigned len, int per ) { return per == 12 ? ( len + 11 ) / 12 : ( len + 7 ) >> 3; }
+
 // vectors of every (src, tile) slice, from the ELL pivots, into rec[].x; rec[].y = length
-__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2 * rec )
+__global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2 * rec, int per )
 {
 	long long const total = (long long)n * ntiles;
 	for( long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x )
@@ -87,7 +92,7 @@ __global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2
 		long long const src = e / ntiles, j = e % ntiles;
 		unsigned const * pv = pivots + src * ( ntiles + 1 ) + j;
 		unsigned const len = pv[1] - pv[0];
-		rec[e] = make_uint2( ( len + 7 ) >> 3, len );
+		rec[e] = make_uint2( slice_vecs( len, per ), len );
 	}
 }
 
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__( 1024 ) slice_offsets( int n, int ntiles, uint
 template <typename Model>
 __global__ void __launch_bounds__( 256 ) slice_fill(
     int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first,
-    unsigned long long const * tile_base, uint2 * rec, unsigned short * slices )
+    unsigned long long const * tile_base, uint2 * rec, unsigned short * slices, int per )
 {
 	using N = typename Model::neuron;
 	snn_info const info{ n };
@@ -158,10 +163,30 @@ __global__ void __launch_bounds__( 256 ) slice_fill(
 		if( r.y == 0 ) continue;
 		int const d0 = tile_first[j], span = tile_first[j + 1] - d0;
 		unsigned const lo = pv[j];
-		unsigned short * out = slices + first * 8;
-		int const padded = (int)( ( r.y + 7 ) & ~7u );
-		for( int e = lane; e < padded; e += 32 )
-			out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
+		if( per == 12 )
+		{
+			// three 10-bit indices per 32-bit word, bits 0-9, 10-19, 20-29
+			unsigned * out = reinterpret_cast<unsigned *>( slices ) + first * 4;
+			int const words = (int)slice_vecs( r.y, 12 ) * 4;
+			for( int w = lane; w < words; w += 32 )
+			{
+				unsigned word = 0;
+				for( int f = 0; f < 3; f++ )
+				{
+					int const e = 3 * w + f;
+					unsigned const x = e < (int)r.y ? (unsigned)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD10;
+					word |= x << ( 10 * f );
+				}
+				out[w] = word;
+			}
+		}
+		else
+		{
+			unsigned short * out = slices + first * 8;
+			int const padded = (int)( ( r.y + 7 ) & ~7u );
+			for( int e = lane; e < padded; e += 32 )
+				out[e] = e < (int)r.y ? (unsigned short)( cls * span + ( row[lo + e] - d0 ) ) : SLICE_PAD;
+		}
 	}
 }
 
@@ -204,7 +229,7 @@ __device__ __forceinline__ void load_counts( net_params const & p, unsigned * cn
 // ------------------------------------------------------------------------------------
 // table[g] = { first vector of the slice, length | vector offset inside its step << 12 }
 __device__ __forceinline__ int ent_len( int2 e ) { return e.y & 0xFFF; }
-__device__ __forceinline__ int ent_vec( int2 e ) { return ( ent_len( e ) + 7 ) >> 3; }
+__device__ __forceinline__ int ent_vec( int2 e, int per ) { return (int)slice_vecs( (unsigned)ent_len( e ), per ); }
 __device__ __forceinline__ int ent_off( int2 e ) { return (int)( (unsigned)e.y >> 12 ); }
 
 // how a staged segment runs
@@ -218,7 +243,7 @@ enum seg_mode
 __device__ __forceinline__ int stage_arrivals(
     net_params const & p, unsigned * cnts, int2 * table, int tile, long long t0, int ks, int L, int * step_begin, int & nent_out, int * scratch );
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int & mode );
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int pack, int & mode );
 
 // Stage the arrivals of the steps [ks, L) of the window starting at t0 (the synchronous
 // path), as many whole steps as fit FLAT_ENT_CAP, and set the segment's mode. Returns the
@@ -236,7 +261,7 @@ __device__ __forceinline__ int stage_table(
 		mode = SEG_DIRECT; // step ks alone exceeds the table
 		return ks + 1;
 	}
-	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, bufv, mode );
+	return stage_offsets( table, ks, ke, nent, step_begin, step_vec, reinterpret_cast<int *>( cnts ), scratch, bufv, p.pack, mode );
 }
 
 // Per-CTA staging of whole steps: the (step, source tile) prefix, then every arrival's
@@ -325,13 +350,13 @@ __device__ __forceinline__ int stage_arrivals(
 // if that is step ks, it runs alone: in pieces, or directly if its offsets do not fit
 // FLAT_P_BITS. Returns the segment's end and sets `mode`.
 __device__ __forceinline__ int stage_offsets(
-    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int & mode )
+    int2 * table, int ks, int ke, int nent, int * step_begin, int * step_vec, int * run_first, int * scratch, int bufv, int pack, int & mode )
 {
 	int const tid = threadIdx.x, nt = blockDim.x;
 	int const per = ( nent + nt - 1 ) / nt;
 	int const g0 = min( nent, tid * per ), g1 = min( nent, g0 + per );
 	int run = 0;
-	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g] );
+	for( int g = g0; g < g1; g++ ) run += ent_vec( table[g], pack );
 	int vtotal;
 	int const my_first = block_exclusive_scan( run, scratch, &vtotal );
 	run_first[tid] = my_first;
@@ -344,7 +369,7 @@ __device__ __forceinline__ int stage_offsets(
 		{
 			int const owner = g / per;
 			v = run_first[owner];
-			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h] );
+			for( int h = owner * per; h < g; h++ ) v += ent_vec( table[h], pack );
 		}
 		step_vec[k] = v;
 	}
@@ -358,7 +383,7 @@ __device__ __forceinline__ int stage_offsets(
 			while( step_begin[k + 1] <= g ) k++;
 			int2 e = table[g];
 			unsigned const rel = (unsigned)( v - step_vec[k] );
-			int const nv = ent_vec( e );
+			int const nv = ent_vec( e, pack );
 			e.y = ent_len( e ) | (int)( ( rel & ( ( 1u << FLAT_P_BITS ) - 1 ) ) << 12 );
 			table[g] = e;
 			v += nv;
@@ -378,7 +403,7 @@ __device__ __forceinline__ int stage_offsets(
 
 // one past the last entry of the piece starting at entry `a` of a step whose entries end
 // at `e`: the entries whose vectors fit one buffer of `bufv` vectors together
-__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv )
+__device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int bufv, int pack )
 {
 	int const pa = ent_off( table[a] );
 	int lo = a, hi = e; // f(g) = off(g) + vec(g) - pa <= bufv holds for g = a
@@ -386,7 +411,7 @@ __device__ __forceinline__ int piece_end( int2 const * table, int a, int e, int 
 	{
 		int const mid = ( lo + hi ) >> 1;
 		int2 const m = table[mid];
-		if( ent_off( m ) + ent_vec( m ) - pa <= bufv )
+		if( ent_off( m ) + ent_vec( m, pack ) - pa <= bufv )
 			lo = mid;
 		else
 			hi = mid;
@@ -430,7 +455,7 @@ __device__ __forceinline__ void issue_piece( net_params const & p, int2 const * 
 	for( int g = a + ( t >> 2 ); g < b; g += groups )
 	{
 		int2 const e = table[g];
-		int const nv = ent_vec( e );
+		int const nv = ent_vec( e, p.pack );
 		uint4 const * src = p.slices + (unsigned)e.x;
 		uint4 * dst = buf + ( ent_off( e ) - pa );
 		for( int j = q; j < nv; j += 4 ) cp_async16( dst + j, src + j );
@@ -441,14 +466,28 @@ __device__ __forceinline__ void count_index( unsigned * cnt, unsigned x )
 {
 	if( x != SLICE_PAD ) atomicAdd( cnt + x, 1u );
 }
-
-// count every index of the `V` vectors in buf, by threads [0, nthreads) of numbering `t`
-__device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned * cnt, int t, int nthreads )
+__device__ __forceinline__ void count_index10( unsigned * cnt, unsigned x )
 {
-#pragma unroll 2
-	for( int v = t; v < V; v += nthreads )
+	if( x != SLICE_PAD10 ) atomicAdd( cnt + x, 1u );
+}
+
+// one counter increment per index of a slice vector (eight 16-bit or twelve 10-bit ones)
+template <int PER>
+__device__ __forceinline__ void count_vector( unsigned * cnt, uint4 const w )
+{
+	if constexpr( PER == 12 )
 	{
-		uint4 const w = buf[v];
+		unsigned const q[4] = { w.x, w.y, w.z, w.w };
+#pragma unroll
+		for( int i = 0; i < 4; i++ )
+		{
+			count_index10( cnt, q[i] & 0x3FFu );
+			count_index10( cnt, ( q[i] >> 10 ) & 0x3FFu );
+			count_index10( cnt, ( q[i] >> 20 ) & 0x3FFu );
+		}
+	}
+	else
+	{
 		count_index( cnt, w.x & 0xFFFFu );
 		count_index( cnt, w.x >> 16 );
 		count_index( cnt, w.y & 0xFFFFu );
@@ -457,6 +496,21 @@ __device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned
 		count_index( cnt, w.z >> 16 );
 		count_index( cnt, w.w & 0xFFFFu );
 		count_index( cnt, w.w >> 16 );
+	}
+}
+
+// count every index of the `V` vectors in buf, by threads [0, nthreads) of numbering `t`
+__device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned * cnt, int t, int nthreads, int pack )
+{
+	if( pack == 12 )
+	{
+#pragma unroll 2
+		for( int v = t; v < V; v += nthreads ) count_vector<12>( cnt, buf[v] );
+	}
+	else
+	{
+#pragma unroll 2
+		for( int v = t; v < V; v += nthreads ) count_vector<8>( cnt, buf[v] );
 	}
 }
 
@@ -712,7 +766,7 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 					for( int g = pt >> 2; g < ea; g += groups )
 					{
 						int2 const e = e1[g];
-						int const nv = ent_vec( e );
+						int const nv = ent_vec( e, p.pack );
 						uint4 const * src = p.slices + (unsigned)e.x;
 						int o = oa + ent_off( e ) + q;
 						if( o >= rb ) o -= rb;
@@ -804,7 +858,7 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 #pragma unroll
 						for( int u = 0; u < 4; u++ )
 						{
-							nv[u] = g + u < eb ? ent_vec( e[u] ) : 0;
+							nv[u] = g + u < eb ? ent_vec( e[u], p.pack ) : 0;
 							sum += nv[u];
 						}
 						int const incl = warp_inclusive_scan( sum );
@@ -874,20 +928,25 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 						{
 							// count the ring region [off, off + V) of step k
 							int const v = m_v[k & 7], o = m_off[k & 7];
-#pragma unroll 2
-							for( int x = tid; x < v; x += ncons )
+							if( p.pack == 12 )
 							{
-								int y = o + x;
-								if( y >= rb ) y -= rb;
-								uint4 const w = ring[y];
-								count_index( cnt, w.x & 0xFFFFu );
-								count_index( cnt, w.x >> 16 );
-								count_index( cnt, w.y & 0xFFFFu );
-								count_index( cnt, w.y >> 16 );
-								count_index( cnt, w.z & 0xFFFFu );
-								count_index( cnt, w.z >> 16 );
-								count_index( cnt, w.w & 0xFFFFu );
-								count_index( cnt, w.w >> 16 );
+#pragma unroll 2
+								for( int x = tid; x < v; x += ncons )
+								{
+									int y = o + x;
+									if( y >= rb ) y -= rb;
+									count_vector<12>( cnt, ring[y] );
+								}
+							}
+							else
+							{
+#pragma unroll 2
+								for( int x = tid; x < v; x += ncons )
+								{
+									int y = o + x;
+									if( y >= rb ) y -= rb;
+									count_vector<8>( cnt, ring[y] );
+								}
 							}
 						}
 						bar_sync_first( ncons ); // counts complete
@@ -945,12 +1004,12 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 						for( int a = step_begin[kk - ks], b = a; b < e; )
 						{
 							a = b;
-							b = piece_end( table, a, e, bufv );
+							b = piece_end( table, a, e, bufv, p.pack );
 							issue_piece( p, table, a, b, buf, tid, nt );
 							cp_async_commit();
 							cp_async_wait_all();
 							__syncthreads();
-							count_buffer( buf, piece_vectors( table, a, b, e, sv ), cnt, tid, nt );
+							count_buffer( buf, piece_vectors( table, a, b, e, sv ), cnt, tid, nt, p.pack );
 							__syncthreads();
 						}
 					}

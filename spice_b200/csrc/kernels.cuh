@@ -64,9 +64,10 @@ struct net_params
 	clock_state * clock;
 	float * dt_ring;
 	int * err;
-	uint4 const * slices;    // tile-major 16-bit slices (window_flat)
+	uint4 const * slices;    // tile-major slices of counter indices (window_flat)
 	uint2 const * slice_rec; // [n][ntiles] { first vector, length } (window_flat)
 	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
+	int pack;                // indices per 16-byte slice vector: 8 (16-bit) or 12 (10-bit)
 	int flat_sync;           // window_flat: every step on the synchronous path
 	long long * done_step;   // [ntiles] last step whose spikes the tile has published
 };

@@ -240,6 +240,7 @@ struct spk_net
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
 	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
+	int pack = 8;           // slice indices per 16-byte vector: 8 (16-bit) or 12 (10-bit)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
 	bool persistent = false; // run() as one cooperative window_flat launch (delay >= 6)
 	std::vector<double> seg_start, seg_cost; // expected work per neuron stretch (tiling)
@@ -275,6 +276,7 @@ struct spk_net
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
 		p.flat_sync = flat_sync;
+		p.pack = pack;
 		p.done_step = done_step.as<long long>();
 		return p;
 	}
@@ -720,7 +722,7 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 // = the SM count for a net alone; fewer for a net that shares the GPU in a batch): the
 // tiles' first neurons and the shared-memory span of the largest tile with inputs; false
 // if the net does not fit window_flat.
-bool plan_flat( int model, int device, long long n, std::vector<cost_segment> const & segs, int target, std::vector<int> & first, int & span )
+bool plan_flat( int model, int device, long long n, std::vector<cost_segment> const & segs, int target, std::vector<int> & first, int & span, int & pack )
 {
 	int optin = 0;
 	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
@@ -734,17 +736,46 @@ bool plan_flat( int model, int device, long long n, std::vector<cost_segment> co
 	int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * attrs + 8 ) ) / 32 * 32 );
 	if( tmax < 128 ) return false;
 	char const * tiling = getenv( "SPK_TILES" );
-	first = ( tiling && !strcmp( tiling, "uniform" ) ) ? uniform_tiles( n, std::min( tmax, 1024 ) )
-	                                                   : balanced_tiles( segs, n, std::max( 1, target ), tmax, tmax_free );
-	if( (int)first.size() >= spk::FLAT_PC ) return false;
+	bool const uniform = tiling && !strcmp( tiling, "uniform" );
+	auto cut = [&]( int tmax_in ) {
+		return uniform ? uniform_tiles( n, std::min( tmax_in, 1024 ) ) : balanced_tiles( segs, n, std::max( 1, target ), tmax_in, tmax_free );
+	};
 	// the largest tile with inputs sets the shared-memory floor (tiles without inputs need
 	// less than it per neuron)
-	span = 0;
-	size_t si = 0;
-	for( size_t i = 0; i + 1 < first.size(); i++ )
+	auto input_span = [&]( std::vector<int> const & f, int tmax_in ) {
+		int sp = 0;
+		size_t si = 0;
+		for( size_t i = 0; i + 1 < f.size(); i++ )
+		{
+			while( si + 1 < segs.size() && segs[si + 1].start <= f[i] ) si++;
+			if( segs[si].cost > UPDATE_COST || f[i + 1] - f[i] <= tmax_in ) sp = std::max( sp, f[i + 1] - f[i] );
+		}
+		return sp;
+	};
+	first = cut( tmax );
+	if( (int)first.size() >= spk::FLAT_PC ) return false;
+	span = input_span( first, tmax );
+	// 10-bit slices (twelve indices per vector instead of eight) when every counter index
+	// fits below SLICE_PAD10: tiles with inputs capped at (SLICE_PAD10 - 1) / classes
+	// neurons, taken if that needs no more tiles (SPK_PACK=16 keeps 16-bit slices)
+	pack = 8;
+	char const * pk = getenv( "SPK_PACK" );
+	int const cap10 = (int)( ( spk::SLICE_PAD10 - 1 ) / std::max( 1, classes ) );
+	if( !( pk && !strcmp( pk, "16" ) ) && cap10 >= 128 )
 	{
-		while( si + 1 < segs.size() && segs[si + 1].start <= first[i] ) si++;
-		if( segs[si].cost > UPDATE_COST || first[i + 1] - first[i] <= tmax ) span = std::max( span, first[i + 1] - first[i] );
+		if( (long long)classes * span < (long long)spk::SLICE_PAD10 )
+			pack = 12;
+		else
+		{
+			std::vector<int> const f10 = cut( std::min( tmax, cap10 ) );
+			int const s10 = input_span( f10, std::min( tmax, cap10 ) );
+			if( f10.size() <= first.size() && (long long)classes * s10 < (long long)spk::SLICE_PAD10 )
+			{
+				first = f10;
+				span = s10;
+				pack = 12;
+			}
+		}
 	}
 	return true;
 }
@@ -753,9 +784,10 @@ bool plan_flat( int model, int device, long long n, std::vector<cost_segment> co
 bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int target )
 {
 	std::vector<int> first;
-	int span = 0;
-	if( !plan_flat( net.model, net.device, net.n, segs, target, first, span ) ) return false;
+	int span = 0, pack = 8;
+	if( !plan_flat( net.model, net.device, net.n, segs, target, first, span, pack ) ) return false;
 	net.flat = true;
+	net.pack = pack;
 	net.flat_tmax = ( span + 31 ) / 32 * 32;
 	net.tc = { spk::FLAT_THREADS, 1, net.flat_tmax, (int)first.size() - 1 };
 	set_tiles( net, first );
@@ -820,7 +852,7 @@ void fill_slices( spk_net & net, dbuf const & bases )
 		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
 		spk::slice_fill<Model><<<blocks, 256, 0, net.stream>>>(
 		    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
-		    bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>() );
+		    bases.as<unsigned long long>(), net.slice_rec.as<uint2>(), net.slices.as<unsigned short>(), net.pack );
 		CK( cudaGetLastError() );
 	}
 }
@@ -835,7 +867,7 @@ void build_slices( spk_net & net )
 	bases.alloc( (size_t)nt * 8 );
 	std::vector<unsigned long long> tot( nt ), base( nt );
 	// vectors per (src, tile) and their per-tile prefix
-	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>() );
+	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>(), net.pack );
 	CK( cudaGetLastError() );
 	spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
 	CK( cudaGetLastError() );
@@ -920,7 +952,7 @@ void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned l
 
 // Upper estimate of the device memory a net of this layout holds once built (the buffers
 // of allocate, build_slices and the plastic state; slices bounded by one 16-byte vector per
-// eight synapses plus one per non-empty (source, tile) pair, at 5 % above the expected
+// 8 or 12 synapses plus one per non-empty (source, tile) pair, at 5 % above the expected
 // synapse count), each buffer rounded up to the allocator's 2 MiB granule.
 size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int device, int tile_target )
 {
@@ -934,12 +966,13 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	int const attrs = describe( model ).neuron_attrs;
 	bool flat = false;
 	long long T = 0;
+	int pack = 8;
 	if( model != SPK_BRUNEL_PLUS )
 	{
 		std::vector<int> first;
 		int span = 0;
 		char const * kern = getenv( "SPK_KERNEL" );
-		if( !( kern && !strcmp( kern, "direct" ) ) && plan_flat( model, device, n, layout_costs( l ), tile_target > 0 ? tile_target : sms, first, span ) )
+		if( !( kern && !strcmp( kern, "direct" ) ) && plan_flat( model, device, n, layout_costs( l ), tile_target > 0 ? tile_target : sms, first, span, pack ) )
 		{
 			flat = true;
 			T = (long long)first.size() - 1;
@@ -965,7 +998,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	if( flat )
 	{
 		b.push_back( (double)n * T * 8 );
-		b.push_back( 16.0 * ( std::ceil( syn / 8 ) + std::min( (double)n * T, syn ) ) );
+		b.push_back( 16.0 * ( std::ceil( syn / pack ) + std::min( (double)n * T, syn ) ) );
 		b.push_back( (double)T * 8 );
 		b.push_back( (double)T * 4 );
 	}
@@ -1439,6 +1472,7 @@ int spk_net_get_info( spk_net * net, spk_net_info * out )
 		out->device_bytes = net->device_bytes();
 		out->kernel_launches = net->kernel_launches;
 		out->persistent = net->persistent ? 1 : 0;
+		out->slice_pack = net->flat ? net->pack : 0;
 	} );
 }
 

@@ -415,3 +415,22 @@ def test_recording_runs_equal_windowed_recording(n, delay, chunks):
         assert bits_equal(x, y)
     for k in range(2 * delay):
         assert np.array_equal(a.step(out=True), b.step(out=True)), k
+
+
+@pytest.mark.parametrize("model,pops,conns,delay", [
+    ("brunel", [20_000, 20_000], [(0, 1, 0.05), (1, 1, 0.05)], 15),
+    ("vogels_abbott", [30_000], [(0, 0, 0.02)], 8),
+    ("synth", [150_000], [(0, 0, 16 / 150_000)], 4),
+])
+def test_ten_bit_slices_match_sixteen_bit(model, pops, conns, delay, monkeypatch):
+    """Slices packed twelve 10-bit indices to a vector against eight 16-bit ones."""
+    layout = Layout(pops, conns)
+    a = Snn(model, layout, delay=delay, seed=6, graph_seed=6)
+    monkeypatch.setenv("SPK_PACK", "16")
+    b = Snn(model, layout, delay=delay, seed=6, graph_seed=6)
+    assert a.info().slice_pack == 12 and b.info().slice_pack == 8
+    ca, ia = a.run_record(300, cap=sum(pops) * 300 // 4)
+    cb, ib = b.run_record(300, cap=sum(pops) * 300 // 4)
+    assert ca.sum() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
