@@ -333,14 +333,6 @@ def batched_specs(count, seed=0):
     return specs
 
 
-def tile_targets(specs, sms):
-    """Tiles per net of a batch: each net's share of the SMs by its expected work
-    (synapses plus a per-neuron update cost), at least one."""
-    work = [s["syn"] * 0.01 + 1000.0 * sum(s["pops"]) for s in specs]
-    total = sum(work)
-    return [max(1, int(round(sms * w / total))) for w in work]
-
-
 def run_batched(args, rank, world):
     """Batched workload: the same nets stepped (a) one at a time, the plain per-job loop
     (spice_bench/paper_plots.cpp:184-231 steps one net after another), and (b) together in
@@ -383,11 +375,23 @@ def run_batched(args, rank, world):
         n.close()
     del plain
 
-    # (b) batch: re-tiled by work share, one Batch
+    # (b) batch: tiles per net by work share at the scale the autotuner measured best
+    from spice_b200.autotune import autotune, layout_work, tile_targets as targets_for
+
+    works = [layout_work(Layout(s["pops"], s["conns"])) for s in specs]
+
+    def build(i, t):
+        n = make(specs[i])
+        n.set_tile_target(t)
+        return n
+
+    t0 = time.perf_counter()
+    scale, tune_times = autotune(build, works, sms, device=dev)
+    tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     nets = [make(s) for s in specs]
     batch = Batch(device=dev)
-    for n, t in zip(nets, tile_targets(specs, sms)):
+    for n, t in zip(nets, targets_for(works, sms, scale)):
         n.set_tile_target(t)
         batch.add(n)
     for n in nets:
@@ -413,7 +417,9 @@ def run_batched(args, rank, world):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"batched_{len(specs)}_nets", "nets": counts, "synapses_total": syn_total,
                            "syn_range": [1e5, 5e7], "bio_s_per_net": steps * DT, "dt": DT, "tiles_total": tiles},
-                "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch},
+                "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch,
+                          "tile_scale": scale, "autotune_s": tune_s,
+                          "autotune_ms_per_step": {str(k): v * 1e3 for k, v in tune_times.items()}},
                 "plain_loop": {"wall_s": wall_plain, "wall_per_bio": wall_plain / bio_total, "setup_s": setup_plain,
                                "wall_s_by_model": per_model,
                                "value": syn_total * steps * DT / wall_plain},

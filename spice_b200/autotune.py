@@ -1,0 +1,81 @@
+"""Tile counts of nets that share the GPU in a batch, and a measured choice among them.
+
+A net alone takes one window_flat CTA per SM. In a batch, every launch runs every tile of
+every net, so the tile count of each net sets both the work per CTA and the number of CTA
+waves per launch. The rule here gives net i a share of the SMs by its expected work,
+
+    tiles_i = max(1, round(scale * sms * work_i / sum(work))),
+
+and `autotune` measures a few scales on the nets themselves (or a sample of them spread
+over their size range) and returns the fastest. Results never depend on the tiling: only
+the speed does.
+"""
+import time
+
+import numpy as np
+
+__all__ = ["layout_work", "tile_targets", "autotune"]
+
+
+def layout_work(layout):
+    """Expected cost of one step of a net: synapses delivered at a nominal rate plus a
+    per-neuron update cost, in the units the tiler of the library uses."""
+    syn = 0.0
+    for s0, s1, d0, d1, p in layout.connections():
+        syn += (s1 - s0) * (d1 - d0) * p
+    return syn * 0.01 + 1000.0 * layout.size()
+
+
+def tile_targets(works, sms, scale=1.0):
+    """Tiles per net: each net's share of `scale * sms` by work, one at least."""
+    total = float(sum(works)) or 1.0
+    return [max(1, int(round(scale * sms * w / total))) for w in works]
+
+
+def _sample(works, max_nets):
+    if len(works) <= max_nets:
+        return list(range(len(works)))
+    order = np.argsort(works)
+    picks = np.linspace(0, len(works) - 1, max_nets).round().astype(int)
+    return sorted(set(int(order[k]) for k in picks))
+
+
+def autotune(build, works, sms, scales=(0.5, 1.0, 2.0, 4.0), steps=150, warmup=30, max_nets=64, device=0):
+    """Measure batch runs of the nets under each tile scale and return
+    (best scale, {scale: seconds per step}).
+
+    build(i, tile_target) -> an unstepped Snn equal to net i of the batch (the caller's
+    constructor with the tile target passed to Snn.set_tile_target or spk_net_create_ex).
+    With more than max_nets nets, a sample spread over their work range is measured, each
+    sampled net with the tiles it would get in the full batch, and the sample's time is
+    scaled by the whole batch's work over the sample's (an estimate: the sample fills fewer
+    SMs than the full batch).
+    """
+    from . import Batch
+
+    idx = _sample(works, max_nets)
+    w_all = float(sum(works)) or 1.0
+    w_sub = float(sum(works[i] for i in idx)) or 1.0
+    times = {}
+    for scale in scales:
+        targets = tile_targets(works, sms, scale)
+        nets = []
+        batch = Batch(device=device)
+        try:
+            for i in idx:
+                net = build(i, targets[i])
+                nets.append(net)
+                batch.add(net)
+            batch.run(warmup)
+            batch.sync()
+            t = time.perf_counter()
+            batch.run(steps)
+            batch.sync()
+            # the sample stands for its share of the whole batch's work
+            times[scale] = (time.perf_counter() - t) / steps * (w_all / w_sub)
+        finally:
+            batch.close()
+            for net in nets:
+                net.close()
+    best = min(times, key=times.get)
+    return best, times

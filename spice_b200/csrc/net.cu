@@ -1050,8 +1050,16 @@ struct spk_batch
 		cudaStream_t stream = nullptr;
 		cudaEvent_t ev = nullptr;
 		dbuf d_params, d_jobs;
-		std::vector<spk::net_params> h_params;
-		std::vector<int4> h_jobs;
+		std::vector<spk::net_params> h_params, c_params; // this run's / on the device
+		std::vector<int4> h_jobs, c_jobs;
+		std::vector<std::pair<int, int>> c_launches; // rounds of the captured graph
+		cudaGraphExec_t graph = nullptr;             // the rounds of the last job table
+		void drop_graph()
+		{
+			if( graph ) cudaGraphExecDestroy( graph );
+			graph = nullptr;
+			c_launches.clear();
+		}
 	};
 	int device = 0;
 	std::vector<spk_net *> nets;
@@ -1062,6 +1070,7 @@ struct spk_batch
 		for( auto * net : nets ) net->batch = nullptr;
 		for( auto & g : groups )
 		{
+			g.drop_graph();
 			if( g.ev ) cudaEventDestroy( g.ev );
 			if( g.stream ) cudaStreamDestroy( g.stream );
 		}
@@ -1126,23 +1135,64 @@ struct spk_batch
 			}
 		}
 		size_t const pb = g.h_params.size() * sizeof( spk::net_params ), jb = g.h_jobs.size() * sizeof( int4 );
-		if( g.d_params.bytes < pb || g.d_jobs.bytes < jb ) CK( cudaStreamSynchronize( g.stream ) ); // launches reading the old ones
+		if( g.d_params.bytes < pb || g.d_jobs.bytes < jb )
+		{
+			CK( cudaStreamSynchronize( g.stream ) ); // launches reading the old ones
+			g.drop_graph();                          // captured the old buffers
+			g.c_params.clear();
+			g.c_jobs.clear();
+		}
 		if( g.d_params.bytes < pb ) g.d_params.alloc( pb );
 		if( g.d_jobs.bytes < jb ) g.d_jobs.alloc( jb );
 		// pageable sources: each copy returns once its source is staged, and the stream
-		// orders it after the previous run's launches that read the same buffers
-		CK( cudaMemcpyAsync( g.d_params.p, g.h_params.data(), pb, cudaMemcpyHostToDevice, g.stream ) );
-		CK( cudaMemcpyAsync( g.d_jobs.p, g.h_jobs.data(), jb, cudaMemcpyHostToDevice, g.stream ) );
-		int const smem = gn[0]->flat_smem;
-		for( auto const & l : launches )
+		// orders it after the previous run's launches that read the same buffers; a table
+		// equal to the one on the device is not sent again
+		auto same = []( auto const & a, auto const & b ) {
+			return a.size() == b.size() && ( a.empty() || !std::memcmp( a.data(), b.data(), a.size() * sizeof( a[0] ) ) );
+		};
+		if( !same( g.h_params, g.c_params ) )
 		{
-			int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
-			switch( model )
+			CK( cudaMemcpyAsync( g.d_params.p, g.h_params.data(), pb, cudaMemcpyHostToDevice, g.stream ) );
+			g.c_params = g.h_params;
+		}
+		if( !same( g.h_jobs, g.c_jobs ) )
+		{
+			CK( cudaMemcpyAsync( g.d_jobs.p, g.h_jobs.data(), jb, cudaMemcpyHostToDevice, g.stream ) );
+			g.c_jobs = g.h_jobs;
+			g.drop_graph();
+		}
+		int const smem = gn[0]->flat_smem;
+		auto launch_all = [&] {
+			for( auto const & l : launches )
 			{
-			case SPK_VOGELS_ABBOTT: launch_model<spice::vogels_abbott>( g, jobs, l.second, smem ); break;
-			case SPK_BRUNEL: launch_model<spice::brunel>( g, jobs, l.second, smem ); break;
-			case SPK_SYNTH: launch_model<spice::synth>( g, jobs, l.second, smem ); break;
+				int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
+				switch( model )
+				{
+				case SPK_VOGELS_ABBOTT: launch_model<spice::vogels_abbott>( g, jobs, l.second, smem ); break;
+				case SPK_BRUNEL: launch_model<spice::brunel>( g, jobs, l.second, smem ); break;
+				case SPK_SYNTH: launch_model<spice::synth>( g, jobs, l.second, smem ); break;
+				}
 			}
+		};
+		// the rounds as one CUDA graph, captured once per job table and round sequence and
+		// replayed by later runs of the same nets and step counts (serving ticks, loops)
+		if( launches.size() < 2 )
+			launch_all();
+		else
+		{
+			if( g.graph && g.c_launches != launches ) g.drop_graph();
+			if( !g.graph )
+			{
+				cudaGraph_t cg;
+				CK( cudaStreamBeginCapture( g.stream, cudaStreamCaptureModeThreadLocal ) );
+				launch_all();
+				CK( cudaStreamEndCapture( g.stream, &cg ) );
+				cudaError_t const e = cudaGraphInstantiate( &g.graph, cg, 0 );
+				cudaGraphDestroy( cg );
+				CK( e );
+				g.c_launches = launches;
+			}
+			CK( cudaGraphLaunch( g.graph, g.stream ) );
 		}
 		for( size_t i = 0; i < gn.size(); i++ )
 		{

@@ -72,3 +72,15 @@ def test_server_and_batch_arguments_checked_without_device(lib):
     assert lib.spk_batch_add(None, None) == spice_b200.ERR_INVALID
     assert lib.spk_server_destroy(None) == spice_b200.OK
     assert lib.spk_batch_destroy(None) == spice_b200.OK
+
+
+def test_tile_targets_share_sms_by_work():
+    from spice_b200.autotune import layout_work, tile_targets
+
+    L = spice_b200.Layout
+    w = [layout_work(L([1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)])), layout_work(L([100], [(0, 0, 0.5)]))]
+    assert w[0] > w[1] > 0
+    t = tile_targets(w, 148)
+    assert t[0] >= t[1] >= 1 and sum(t) <= 150
+    assert tile_targets(w, 148, 2.0)[0] > t[0]
+    assert tile_targets([0.0, 0.0], 148) == [1, 1]

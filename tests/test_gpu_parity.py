@@ -337,8 +337,12 @@ def test_batch_matches_nets_alone():
     batch.run(101)
     for a in alone:
         a.run(101)
+    for _ in range(3):  # equal job tables: the captured rounds replayed
+        batch.run(30)
+    for a in alone:
+        a.run(90)
     for a, b in zip(alone, batched):
-        assert a.info().steps == b.info().steps == 141
+        assert a.info().steps == b.info().steps == 231
         for x, y in zip(a.neurons(), b.neurons()):
             assert bits_equal(x, y)
         for x, y in zip(a.synapses(), b.synapses()):
@@ -347,10 +351,10 @@ def test_batch_matches_nets_alone():
             assert np.array_equal(a.step(out=True), b.step(out=True)), k
     batch.remove(batched[0])
     batch.run(5)
-    assert batched[0].info().steps == 141 + 2 * batched[0].delay()
+    assert batched[0].info().steps == 231 + 2 * batched[0].delay()
     batched[1].close()  # a destroyed net leaves its batch
     batch.run(2)
-    assert batched[2].info().steps == 141 + 2 * batched[2].delay() + 5 + 2
+    assert batched[2].info().steps == 231 + 2 * batched[2].delay() + 5 + 2
     batch.close()
 
 
@@ -434,3 +438,18 @@ def test_ten_bit_slices_match_sixteen_bit(model, pops, conns, delay, monkeypatch
     assert ca.sum() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
     for x, y in zip(a.neurons(), b.neurons()):
         assert bits_equal(x, y)
+
+
+def test_autotune_measures_every_scale():
+    from spice_b200.autotune import autotune, layout_work
+
+    lays = [Layout([n, n], [(0, 1, 0.1), (1, 1, 0.1)]) for n in (500, 1500, 4000)]
+    works = [layout_work(l) for l in lays]
+
+    def build(i, t):
+        net = Snn("brunel", lays[i], delay=15, seed=i + 1)
+        net.set_tile_target(t)
+        return net
+
+    best, times = autotune(build, works, 148, scales=(0.5, 2.0), steps=45, warmup=15)
+    assert best in (0.5, 2.0) and set(times) == {0.5, 2.0} and all(v > 0 for v in times.values())
