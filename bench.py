@@ -386,12 +386,12 @@ def run_batched(args, rank, world):
         return n
 
     t0 = time.perf_counter()
-    scale, tune_times = autotune(build, works, sms, device=dev)
+    scale, buckets, tune_times = autotune(build, works, sms, device=dev)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     nets = [make(s) for s in specs]
     batch = Batch(device=dev)
-    for n, t in zip(nets, targets_for(works, sms, scale)):
+    for n, t in zip(nets, targets_for(works, sms, scale, buckets)):
         n.set_tile_target(t)
         batch.add(n)
     for n in nets:
@@ -419,7 +419,7 @@ def run_batched(args, rank, world):
                            "syn_range": [1e5, 5e7], "bio_s_per_net": steps * DT, "dt": DT, "tiles_total": tiles},
                 "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch,
                           "tile_scale": scale, "autotune_s": tune_s,
-                          "autotune_ms_per_step": {str(k): v * 1e3 for k, v in tune_times.items()}},
+                          "autotune_ms_per_step": {k: v * 1e3 for k, v in tune_times.items()}},
                 "plain_loop": {"wall_s": wall_plain, "wall_per_bio": wall_plain / bio_total, "setup_s": setup_plain,
                                "wall_s_by_model": per_model,
                                "value": syn_total * steps * DT / wall_plain},
@@ -464,6 +464,7 @@ def run_serving(args, rank, world):
     torch.cuda.set_device(dev)
     jobs = serving_jobs(args.rate, args.duration)
     work = sum(j["syn"] * j["steps"] * DT for j in jobs)
+    syn_steps = sum(j["syn"] * j["steps"] for j in jobs)  # synapse updates: every synapse every step
 
     def pct(x, q):
         return float(np.percentile(np.asarray(x), q)) if x else None
@@ -519,10 +520,13 @@ def run_serving(args, rank, world):
                            "syn_range": [1e6, 2e8], "bio_range_s": [0.1, 2.0], "arrival_s": args.duration,
                            "budget_gb": args.budget_gb, "quantum_steps": args.quantum},
                 "server": {"p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "span_s": span, "done": states.count(2),
+                           "sims_per_s": states.count(2) / span, "synapse_steps_per_s": syn_steps / span,
                            "peak_gb": st["peak_bytes"] / 1e9, "ticks": st["ticks"],
                            "build_s": st["build_seconds"], "tick_s": st["tick_seconds"]},
                 "plain_loop": {"p50_s": pct(lat_plain, 50), "p99_s": pct(lat_plain, 99), "span_s": span_plain,
-                               "value": work / span_plain, "build_s": build_plain, "run_s_by_model": run_plain},
+                               "value": work / span_plain, "sims_per_s": len(jobs) / span_plain,
+                               "synapse_steps_per_s": syn_steps / span_plain, "build_s": build_plain,
+                               "run_s_by_model": run_plain},
                 "speedup_vs_plain_loop": span_plain / span, "clocks": clk}
         print(json.dumps(line), flush=True)
 

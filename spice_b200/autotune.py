@@ -4,17 +4,18 @@ A net alone takes one window_flat CTA per SM. In a batch, every launch runs ever
 every net, so the tile count of each net sets both the work per CTA and the number of CTA
 waves per launch. The rule here gives net i a share of the SMs by its expected work,
 
-    tiles_i = max(1, round(scale * sms * work_i / sum(work))),
+    tiles_i = max(1, round(scale_b * sms * work_i / sum(work))),
 
-and `autotune` measures a few scales on the nets themselves (or a sample of them spread
-over their size range) and returns the fastest. Results never depend on the tiling: only
-the speed does.
+with one scale per size bucket b (nets split into buckets by work), and `autotune`
+measures scales on the nets themselves (or a sample of them spread over their size range):
+first one scale for all, then each bucket's scale in turn with the others held. Results
+never depend on the tiling: only the speed does.
 """
 import time
 
 import numpy as np
 
-__all__ = ["layout_work", "tile_targets", "autotune"]
+__all__ = ["layout_work", "tile_targets", "size_buckets", "autotune"]
 
 
 def layout_work(layout):
@@ -26,10 +27,22 @@ def layout_work(layout):
     return syn * 0.01 + 1000.0 * layout.size()
 
 
-def tile_targets(works, sms, scale=1.0):
-    """Tiles per net: each net's share of `scale * sms` by work, one at least."""
+def tile_targets(works, sms, scale=1.0, buckets=None):
+    """Tiles per net: each net's share of `scale * sms` by work, one at least. `scale` may
+    be a list, one per bucket, with buckets[i] the bucket of net i."""
     total = float(sum(works)) or 1.0
-    return [max(1, int(round(scale * sms * w / total))) for w in works]
+    if buckets is None:
+        return [max(1, int(round(scale * sms * w / total))) for w in works]
+    return [max(1, int(round(scale[b] * sms * w / total))) for w, b in zip(works, buckets)]
+
+
+def size_buckets(works, count=3):
+    """Bucket of each net: equal-sized groups by work, smallest first."""
+    order = np.argsort(works, kind="stable")
+    out = [0] * len(works)
+    for rank, i in enumerate(order):
+        out[int(i)] = min(count - 1, rank * count // max(1, len(works)))
+    return out
 
 
 def _sample(works, max_nets):
@@ -40,9 +53,34 @@ def _sample(works, max_nets):
     return sorted(set(int(order[k]) for k in picks))
 
 
-def autotune(build, works, sms, scales=(0.5, 1.0, 2.0, 4.0), steps=150, warmup=30, max_nets=64, device=0):
-    """Measure batch runs of the nets under each tile scale and return
-    (best scale, {scale: seconds per step}).
+def _measure(build, idx, targets, w_all, steps, warmup, device):
+    from . import Batch
+
+    nets = []
+    batch = Batch(device=device)
+    try:
+        for i in idx:
+            net = build(i, targets[i])
+            nets.append(net)
+            batch.add(net)
+        batch.run(warmup)
+        batch.sync()
+        t = time.perf_counter()
+        batch.run(steps)
+        batch.sync()
+        return time.perf_counter() - t
+    finally:
+        batch.close()
+        for net in nets:
+            net.close()
+
+
+def autotune(build, works, sms, scales=(0.5, 1.0, 2.0, 4.0), nbuckets=3, steps=150, warmup=30, max_nets=64, device=0):
+    """Measure batch runs of the nets under tile scales and return
+    (per-bucket scales, buckets of the nets, {description: seconds per step}).
+
+    First every candidate scale for all buckets at once; then, from the best, each bucket's
+    scale in turn over the candidates with the other buckets held.
 
     build(i, tile_target) -> an unstepped Snn equal to net i of the batch (the caller's
     constructor with the tile target passed to Snn.set_tile_target or spk_net_create_ex).
@@ -51,31 +89,23 @@ def autotune(build, works, sms, scales=(0.5, 1.0, 2.0, 4.0), steps=150, warmup=3
     scaled by the whole batch's work over the sample's (an estimate: the sample fills fewer
     SMs than the full batch).
     """
-    from . import Batch
-
     idx = _sample(works, max_nets)
+    buckets = size_buckets(works, nbuckets)
     w_all = float(sum(works)) or 1.0
     w_sub = float(sum(works[i] for i in idx)) or 1.0
     times = {}
-    for scale in scales:
-        targets = tile_targets(works, sms, scale)
-        nets = []
-        batch = Batch(device=device)
-        try:
-            for i in idx:
-                net = build(i, targets[i])
-                nets.append(net)
-                batch.add(net)
-            batch.run(warmup)
-            batch.sync()
-            t = time.perf_counter()
-            batch.run(steps)
-            batch.sync()
-            # the sample stands for its share of the whole batch's work
-            times[scale] = (time.perf_counter() - t) / steps * (w_all / w_sub)
-        finally:
-            batch.close()
-            for net in nets:
-                net.close()
-    best = min(times, key=times.get)
-    return best, times
+
+    def run(sc):
+        key = "/".join(f"{x:g}" for x in sc)
+        if key not in times:
+            t = _measure(build, idx, tile_targets(works, sms, sc, buckets), w_all, steps, warmup, device)
+            times[key] = t / steps * (w_all / w_sub)
+        return times[key]
+
+    best = min(([s] * nbuckets for s in scales), key=run)
+    for b in range(nbuckets):
+        if not any(buckets[i] == b for i in idx):
+            continue
+        cands = [best[:b] + [s] + best[b + 1:] for s in scales]
+        best = min(cands, key=run)
+    return best, buckets, times

@@ -84,3 +84,7 @@ def test_tile_targets_share_sms_by_work():
     assert t[0] >= t[1] >= 1 and sum(t) <= 150
     assert tile_targets(w, 148, 2.0)[0] > t[0]
     assert tile_targets([0.0, 0.0], 148) == [1, 1]
+    from spice_b200.autotune import size_buckets
+
+    assert size_buckets([5.0, 1.0, 3.0], 3) == [2, 0, 1]
+    assert tile_targets(w, 148, [1.0, 4.0], [0, 1])[1] >= t[1]

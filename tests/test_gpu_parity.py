@@ -451,5 +451,6 @@ def test_autotune_measures_every_scale():
         net.set_tile_target(t)
         return net
 
-    best, times = autotune(build, works, 148, scales=(0.5, 2.0), steps=45, warmup=15)
-    assert best in (0.5, 2.0) and set(times) == {0.5, 2.0} and all(v > 0 for v in times.values())
+    best, buckets, times = autotune(build, works, 148, scales=(0.5, 2.0), nbuckets=3, steps=45, warmup=15)
+    assert len(best) == 3 and all(s in (0.5, 2.0) for s in best) and sorted(buckets) == [0, 1, 2]
+    assert "0.5/0.5/0.5" in times and "2/2/2" in times and all(v > 0 for v in times.values())
