@@ -197,6 +197,18 @@ int spk_net_adj( spk_net * net, int32_t * out, uint64_t cap );
 int spk_net_neurons( spk_net * net, void * const * attrs );
 int spk_net_synapses( spk_net * net, void * const * attrs );
 
+/* Checkpoints. The reference's snapshot is adj() + neurons() + synapses() and the
+ * conversion constructor (spice/cuda/snn.d.cpp:123-143), which drops the spikes in flight
+ * and the lazy-STDP history. A checkpoint keeps everything a net needs to continue bit
+ * for bit: edges, neuron state, the spike ring and its publication flags, the simulated
+ * clock and, for Brunel+, the lazy-STDP state; derived tables are rebuilt on restore.
+ * spk_net_checkpoint with buf == NULL returns the size in *out_bytes; otherwise it writes
+ * that many bytes (SPK_ERR_INVALID if cap is smaller). spk_net_restore makes a new net on
+ * `device` that continues where the saved one stood (same tiling; the checkpoint is
+ * validated before any device work). */
+int spk_net_checkpoint( spk_net * net, void * buf, uint64_t cap, uint64_t * out_bytes );
+int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device );
+
 /* Attribute counts of a model's neuron and synapse tuples (as exported above) and, per
  * attribute, 'f' (float32) or 'i' (int32) in types (neuron attributes, then synapse). */
 int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs, char * types, int types_cap );

@@ -127,6 +127,8 @@ def library():
         "spk_net_synapses": (I, [VP, P(VP)]),
         "spk_model_attrs": (I, [I, P(I), P(I), C.c_char_p, I]),
         "spk_net_set_tile_target": (I, [VP, I]),
+        "spk_net_checkpoint": (I, [VP, VP, U64, P(U64)]),
+        "spk_net_restore": (I, [P(VP), VP, U64, I]),
         "spk_net_create_ex": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I, I]),
         "spk_net_estimate_bytes": (I, [I, P(_LayoutDesc), I, I, I, P(U64)]),
         "spk_batch_run_nets": (I, [VP, I, P(VP), P(U64)]),
@@ -359,6 +361,27 @@ class Snn:
     def set_synapses(self, arrays):
         arrs = [np.ascontiguousarray(a, dtype=t) for a, t in zip(arrays, self._sdt)]
         _check(library().spk_net_set_synapses(self._h, _arr_ptrs(arrs)))
+
+    def checkpoint(self):
+        """Everything the net needs to continue bit for bit (bytes): edges, state, the spike
+        ring, the clock and the lazy-STDP state. Snn.restore(data) continues from it."""
+        lib = library()
+        size = C.c_uint64()
+        _check(lib.spk_net_checkpoint(self._h, None, 0, C.byref(size)))
+        buf = np.empty(size.value, dtype=np.uint8)
+        _check(lib.spk_net_checkpoint(self._h, buf.ctypes.data, buf.size, C.byref(size)))
+        return buf.tobytes()
+
+    @classmethod
+    def restore(cls, data, device=0):
+        """A new net continuing from checkpoint() bytes."""
+        net = cls.__new__(cls)
+        net._h = C.c_void_p()
+        arr = np.frombuffer(data, dtype=np.uint8)
+        _check(library().spk_net_restore(C.byref(net._h), arr.ctypes.data, arr.size, int(device)))
+        net.model = MODEL_NAMES[net.info().model]
+        net._ndt, net._sdt = model_attrs(net.model)
+        return net
 
     def set_tile_target(self, target):
         """Re-tile (before the first step) into about `target` tiles, for sharing the GPU."""

@@ -795,6 +795,8 @@ bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int tar
 }
 
 // buffers + pivots; edges must be filled before build_pivots is enqueued
+void allocate_buffers( spk_net & net );
+
 void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs, int tile_target = 0 )
 {
 	require( n > 0 && n <= INT_MAX, "invalid neuron count" );
@@ -821,9 +823,18 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	char const * kern = getenv( "SPK_KERNEL" );
 	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, tile_target > 0 ? tile_target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
+	net.ring_slots = 2 * net.delay;
+	allocate_buffers( net );
+}
+
+// every per-net buffer for the net's size, tiling and ring (edges, pivots, ring, clock,
+// neuron state, gather buffers, plastic state), then the kernels' configuration
+void allocate_buffers( spk_net & net )
+{
+	long long const n = net.n, width = net.width;
+	model_desc const md = describe( net.model );
 	net.edges.alloc( (size_t)( n * width ) * 4 );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
-	net.ring_slots = 2 * net.delay;
 	net.ring_ids.alloc( (size_t)net.ring_slots * n * 4 );
 	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4 );
 	net.clock.alloc( sizeof( spk::clock_state ) );
@@ -1016,6 +1027,50 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	double total = 0;
 	for( double x : b ) total += std::ceil( x / granule ) * granule;
 	return (size_t)total;
+}
+
+// ------------------------------------------------------------------------------------
+// checkpoints: everything a net needs to continue bit for bit, in host memory
+// ------------------------------------------------------------------------------------
+// Layout: ckpt_header, tile_first[ntiles + 1] (int32), then per buffer { u32 id, u64 bytes,
+// bytes }. Derived buffers (pivots, slices, slice records) are rebuilt from the edges and
+// tiles on restore; the spike ring, clock and (Brunel+) the lazy-STDP state are kept, so
+// spikes in flight and pending weight updates survive.
+struct ckpt_header
+{
+	char magic[8];
+	uint32_t version;
+	int32_t model;
+	int64_t n, width;
+	int32_t delay;
+	float dt;
+	uint64_t seed, steps;
+	int32_t ntiles, flat, pack, ring_slots, flat_tmax, threads, npt, tile;
+	int32_t nbufs, reserved;
+};
+constexpr char CKPT_MAGIC[8] = { 'S', 'P', 'K', 'C', 'K', 'P', 'T', '1' };
+
+// the checkpointed buffers of a net, by id (the same order on save and restore)
+std::vector<std::pair<uint32_t, void *>> ckpt_buffers( spk_net & net )
+{
+	std::vector<std::pair<uint32_t, void *>> b;
+	auto add = [&]( uint32_t id, auto & buf ) { b.push_back( { id, static_cast<void *>( &buf ) } ); };
+	add( 1, net.edges );
+	for( int i = 0; i < describe( net.model ).neuron_attrs; i++ ) add( 10 + i, net.attr[i] );
+	add( 20, net.ring_ids );
+	add( 21, net.ring_cnt );
+	add( 22, net.clock );
+	add( 23, net.dt_ring );
+	if( net.flat ) add( 24, net.done_step );
+	return b;
+}
+std::vector<std::pair<uint32_t, spk::plastic_state::buf *>> ckpt_plastic( spk_net & net )
+{
+	auto & q = net.plast;
+	if( net.model != SPK_BRUNEL_PLUS ) return {};
+	return { { 40, &q.W },        { 41, &q.za },         { 42, &q.zpre },       { 43, &q.zpost },     { 44, &q.hist },
+	         { 45, &q.rf_a },     { 46, &q.zrf_a },      { 47, &q.rf_c },       { 48, &q.zrf_c },     { 49, &q.ring_meta },
+	         { 50, &q.flush_ring }, { 51, &q.flush_cnt }, { 52, &q.ring_pot } };
 }
 
 spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int device )
@@ -1564,6 +1619,134 @@ int spk_net_synapses( spk_net * net, void * const * attrs )
 		    net->params(), static_cast<float *>( attrs[0] ), static_cast<float *>( attrs[1] ), static_cast<float *>( attrs[2] ), net->sms,
 		    net->stream ) );
 		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
+
+int spk_net_checkpoint( spk_net * net, void * buf, uint64_t cap, uint64_t * out_bytes )
+{
+	return guarded( [&] {
+		require( net != nullptr && out_bytes != nullptr, "null argument" );
+		device_guard g( net->device );
+		net->sync(); // every queued step launched, and no device error
+		auto const bufs = ckpt_buffers( *net );
+		auto const pl = ckpt_plastic( *net );
+		uint64_t total = sizeof( ckpt_header ) + ( net->tile_first_host.size() ) * 4;
+		for( auto const & x : bufs ) total += 12 + static_cast<dbuf *>( x.second )->bytes;
+		for( auto const & x : pl ) total += 12 + x.second->bytes;
+		*out_bytes = total;
+		if( buf == nullptr ) return; // size query
+		require( cap >= total, "checkpoint buffer too small" );
+		ckpt_header h{};
+		std::memcpy( h.magic, CKPT_MAGIC, 8 );
+		h.version = 1;
+		h.model = net->model;
+		h.n = net->n;
+		h.width = net->width;
+		h.delay = net->delay;
+		h.dt = net->dt;
+		h.seed = net->seed;
+		h.steps = net->steps;
+		h.ntiles = net->tc.ntiles;
+		h.flat = net->flat ? 1 : 0;
+		h.pack = net->pack;
+		h.ring_slots = net->ring_slots;
+		h.flat_tmax = net->flat_tmax;
+		h.threads = net->tc.threads;
+		h.npt = net->tc.npt;
+		h.tile = net->tc.tile;
+		h.nbufs = (int32_t)( bufs.size() + pl.size() );
+		unsigned char * o = static_cast<unsigned char *>( buf );
+		std::memcpy( o, &h, sizeof h );
+		o += sizeof h;
+		std::memcpy( o, net->tile_first_host.data(), net->tile_first_host.size() * 4 );
+		o += net->tile_first_host.size() * 4;
+		auto put = [&]( uint32_t id, void const * dev, uint64_t bytes ) {
+			std::memcpy( o, &id, 4 );
+			std::memcpy( o + 4, &bytes, 8 );
+			o += 12;
+			if( bytes ) CK( cudaMemcpy( o, dev, bytes, cudaMemcpyDeviceToHost ) );
+			o += bytes;
+		};
+		for( auto const & x : bufs ) put( x.first, static_cast<dbuf *>( x.second )->p, static_cast<dbuf *>( x.second )->bytes );
+		for( auto const & x : pl ) put( x.first, x.second->p, x.second->bytes );
+	} );
+}
+
+int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device )
+{
+	return guarded( [&] {
+		require( out != nullptr && buf != nullptr, "null argument" );
+		*out = nullptr;
+		require( size >= sizeof( ckpt_header ), "checkpoint truncated" );
+		ckpt_header h;
+		std::memcpy( &h, buf, sizeof h );
+		require( !std::memcmp( h.magic, CKPT_MAGIC, 8 ) && h.version == 1, "not a checkpoint of this library" );
+		describe( h.model );
+		require( h.n > 0 && h.n <= INT_MAX && h.width >= 0 && h.width % 32 == 0 && h.delay >= 1 && h.ntiles >= 1 &&
+		             h.ring_slots >= 2 * h.delay && ( h.pack == 8 || h.pack == 12 ),
+		         "checkpoint header is inconsistent" );
+		uint64_t const tiles_bytes = (uint64_t)( h.ntiles + 1 ) * 4;
+		require( size >= sizeof h + tiles_bytes, "checkpoint truncated" );
+		unsigned char const * in = static_cast<unsigned char const *>( buf ) + sizeof h;
+		std::vector<int> first( h.ntiles + 1 );
+		std::memcpy( first.data(), in, tiles_bytes );
+		in += tiles_bytes;
+		require( first[0] == 0 && first[h.ntiles] == h.n, "checkpoint tiling is inconsistent" );
+		for( int i = 0; i < h.ntiles; i++ ) require( first[i] < first[i + 1], "checkpoint tiling is inconsistent" );
+		// read the buffer directory first: every size checked before any device work
+		std::vector<std::tuple<uint32_t, uint64_t, unsigned char const *>> dir;
+		unsigned char const * end = static_cast<unsigned char const *>( buf ) + size;
+		for( int b = 0; b < h.nbufs; b++ )
+		{
+			require( end - in >= 12, "checkpoint truncated" );
+			uint32_t id;
+			uint64_t bytes;
+			std::memcpy( &id, in, 4 );
+			std::memcpy( &bytes, in + 4, 8 );
+			in += 12;
+			require( (uint64_t)( end - in ) >= bytes, "checkpoint truncated" );
+			dir.emplace_back( id, bytes, in );
+			in += bytes;
+		}
+
+		std::unique_ptr<spk_net> net( new_net( h.model, h.dt, h.delay, h.seed, device ) );
+		device_guard g( device );
+		net->n = h.n;
+		net->width = h.width;
+		CK( cudaDeviceGetAttribute( &net->sms, cudaDevAttrMultiProcessorCount, device ) );
+		net->flat = h.flat != 0;
+		net->pack = h.pack;
+		net->flat_tmax = h.flat_tmax;
+		net->tc = { h.threads, h.npt, h.tile, h.ntiles };
+		set_tiles( *net, first );
+		net->ring_slots = h.ring_slots;
+		allocate_buffers( *net );
+		auto find = [&]( uint32_t id, uint64_t bytes ) -> unsigned char const * {
+			for( auto const & d : dir )
+				if( std::get<0>( d ) == id )
+				{
+					require( std::get<1>( d ) == bytes, "checkpoint buffer size differs from the net's" );
+					return std::get<2>( d );
+				}
+			throw spk_error( SPK_ERR_INVALID, "checkpoint lacks a buffer" );
+		};
+		// edges first: the pivots and slices are rebuilt from them (which resets the
+		// publication flags), then the state over them
+		dbuf & e = net->edges;
+		if( e.bytes ) CK( cudaMemcpy( e.p, find( 1, e.bytes ), e.bytes, cudaMemcpyHostToDevice ) );
+		enqueue_pivots( *net );
+		CK( cudaStreamSynchronize( net->stream ) );
+		for( auto const & x : ckpt_buffers( *net ) )
+		{
+			dbuf & d = *static_cast<dbuf *>( x.second );
+			if( x.first == 1 || d.bytes == 0 ) continue;
+			CK( cudaMemcpy( d.p, find( x.first, d.bytes ), d.bytes, cudaMemcpyHostToDevice ) );
+		}
+		for( auto const & x : ckpt_plastic( *net ) )
+			if( x.second->bytes ) CK( cudaMemcpy( x.second->p, find( x.first, x.second->bytes ), x.second->bytes, cudaMemcpyHostToDevice ) );
+		net->steps = net->launched = h.steps;
+		net->configure();
+		*out = net.release();
 	} );
 }
 

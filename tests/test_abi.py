@@ -88,3 +88,15 @@ def test_tile_targets_share_sms_by_work():
 
     assert size_buckets([5.0, 1.0, 3.0], 3) == [2, 0, 1]
     assert tile_targets(w, 148, [1.0, 4.0], [0, 1])[1] >= t[1]
+
+
+def test_restore_rejects_bad_checkpoints_before_device_work(lib):
+    import ctypes as C
+
+    h = C.c_void_p()
+    junk = (C.c_ubyte * 256)()
+    assert lib.spk_net_restore(C.byref(h), junk, 256, 0) == spice_b200.ERR_INVALID
+    assert b"not a checkpoint" in lib.spk_last_error()
+    assert lib.spk_net_restore(C.byref(h), junk, 8, 0) == spice_b200.ERR_INVALID
+    assert b"truncated" in lib.spk_last_error()
+    assert lib.spk_net_checkpoint(None, None, 0, None) == spice_b200.ERR_INVALID

@@ -454,3 +454,32 @@ def test_autotune_measures_every_scale():
     best, buckets, times = autotune(build, works, 148, scales=(0.5, 2.0), nbuckets=3, steps=45, warmup=15)
     assert len(best) == 3 and all(s in (0.5, 2.0) for s in best) and sorted(buckets) == [0, 1, 2]
     assert "0.5/0.5/0.5" in times and "2/2/2" in times and all(v > 0 for v in times.values())
+
+
+# ----------------------------------------------------------------------- checkpoints
+@pytest.mark.parametrize("model,pops,conns,delay,first", [
+    ("brunel", [20_000, 20_000], [(0, 1, 0.05), (1, 1, 0.05)], 15, 337),        # persistent window_flat
+    ("vogels_abbott", [4000], [(0, 0, 0.02)], 1, 123),                           # delay 1: windows of one step
+    ("brunel_with_plasticity", [1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 211),  # lazy STDP state
+    ("synth", [200_000], [(0, 0, 16 / 200_000)], 8, 96),
+])
+def test_checkpoint_restore_continues_bit_for_bit(model, pops, conns, delay, first):
+    """A net restored from a checkpoint (spikes in flight, clock, lazy-STDP state) continues
+    exactly as the original does."""
+    a = Snn(model, Layout(pops, conns), delay=delay, seed=9, graph_seed=9)
+    a.run(first)
+    if model == "brunel":
+        a.run_record(200, cap=sum(pops) * 200)  # an enlarged spike ring travels too
+    data = a.checkpoint()
+    b = Snn.restore(data)
+    assert b.info().steps == a.info().steps and b.num_neurons() == a.num_neurons()
+    ca, ia = a.run_record(2 * delay + 50, cap=sum(pops) * 100)
+    cb, ib = b.run_record(2 * delay + 50, cap=sum(pops) * 100)
+    assert ca.sum() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    a.run(300)
+    b.run(300)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+    for x, y in zip(a.synapses(), b.synapses()):
+        assert bits_equal(x, y)
+    assert np.array_equal(a.adj()[0], b.adj()[0])
