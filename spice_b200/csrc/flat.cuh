@@ -6,10 +6,11 @@
 // Data layout ("slices"). Besides the ELL rows, the net keeps every row's part inside
 // every tile as a slice of counter indices, class(src) * span + (target - d0), padded to a
 // whole 16-byte vector: eight 16-bit indices per vector (pad SLICE_PAD), or, when every
-// index of the net fits 10 bits, twelve (three per 32-bit word, pad SLICE_PAD10). A tile's slices lie contiguously in
-// ascending source order, and rec[src * ntiles + tile] = { first vector, length }. So a
-// CTA reads only its own tile's region, two bytes per synapse, already in the form its
-// counters are indexed by.
+// index of the net fits 10 bits, twelve (three per 32-bit word, pad SLICE_PAD10). A row's
+// slices lie contiguously in tile order (source-major), and rec[src * ntiles + tile] =
+// { first vector, length }. A CTA reads 1.33 or 2 bytes per synapse, already in the form
+// its counters are indexed by; and since all tiles fetch their slices of the same spiking
+// rows at about the same time, each row is one contiguous stretch of DRAM.
 //
 // All arrivals of a window fired before it started, so a step's arrivals can be prepared
 // steps ahead. The CTA splits into FLAT_PRODUCERS producer warps and consumer warps. While
@@ -96,55 +97,41 @@ __global__ void slice_vectors( int n, int ntiles, unsigned const * pivots, uint2
 	}
 }
 
-// per tile (one CTA of 1024 threads each): rec[src][tile].x <- exclusive prefix over src
-// of the vector counts (tile-relative), totals[tile] <- the tile's vectors
-__global__ void __launch_bounds__( 1024 ) slice_offsets( int n, int ntiles, uint2 * rec, unsigned long long * totals )
+// one warp per source row: rec[src][tile].x <- exclusive prefix over the row's tiles of the
+// vector counts (row-relative), row_vectors[src] <- the row's vectors; tile_inputs[tile]
+// <- 1 if any row has synapses in the tile
+__global__ void slice_row_offsets( int n, int ntiles, uint2 * rec, unsigned * row_vectors, int * tile_inputs )
 {
-	__shared__ unsigned long long s_run[1024];
-	int const j = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
-	long long const per = ( (long long)n + nt - 1 ) / nt;
-	long long const s0 = min( (long long)n, tid * per ), s1 = min( (long long)n, s0 + per );
-	unsigned long long run = 0;
-	for( long long s = s0; s < s1; s++ ) run += rec[s * ntiles + j].x;
-	s_run[tid] = run;
-	__syncthreads();
-	if( tid < 32 )
+	int const warp = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5, lane = threadIdx.x & 31;
+	if( warp >= n ) return;
+	uint2 * r = rec + (long long)warp * ntiles;
+	unsigned carry = 0;
+	for( int j0 = 0; j0 < ntiles; j0 += 32 )
 	{
-		// 64-bit exclusive scan of the per-thread sums: lane l owns nt / 32 consecutive ones
-		int const chunk = nt / 32;
-		unsigned long long acc = 0;
-		for( int i = 0; i < chunk; i++ ) acc += s_run[tid * chunk + i];
-		unsigned long long incl = acc;
+		int const j = j0 + lane;
+		uint2 const e = j < ntiles ? r[j] : make_uint2( 0u, 0u );
+		unsigned incl = e.x;
 		for( int o = 1; o < 32; o <<= 1 )
 		{
-			unsigned long long const y = __shfl_up_sync( 0xffffffffu, incl, o );
-			if( tid >= o ) incl += y;
+			unsigned const y = __shfl_up_sync( 0xffffffffu, incl, o );
+			if( lane >= o ) incl += y;
 		}
-		unsigned long long base = incl - acc;
-		for( int i = 0; i < chunk; i++ )
+		if( j < ntiles )
 		{
-			unsigned long long const v = s_run[tid * chunk + i];
-			s_run[tid * chunk + i] = base;
-			base += v;
+			r[j].x = carry + incl - e.x;
+			if( e.y && !*(int volatile *)( tile_inputs + j ) ) atomicOr( tile_inputs + j, 1 );
 		}
-		if( tid == 31 ) totals[j] = incl;
+		carry += __shfl_sync( 0xffffffffu, incl, 31 );
 	}
-	__syncthreads();
-	unsigned long long off = s_run[tid];
-	for( long long s = s0; s < s1; s++ )
-	{
-		uint2 & r = rec[s * ntiles + j];
-		unsigned const v = r.x;
-		r.x = (unsigned)off;
-		off += v;
-	}
+	if( lane == 0 ) row_vectors[warp] = carry;
 }
 
-// one warp per source row: rebase rec[] to global vector indices and write every slice
+// one warp per source row: rebase rec[] to global vector indices (the row's first vector
+// row_base[src] plus the row-relative offset) and write every slice
 template <typename Model>
 __global__ void __launch_bounds__( 256 ) slice_fill(
     int n, int width, int ntiles, int const * edges, unsigned const * pivots, int const * tile_first,
-    unsigned long long const * tile_base, uint2 * rec, unsigned short * slices, int per )
+    unsigned long long const * row_base, uint2 * rec, unsigned short * slices, int per )
 {
 	using N = typename Model::neuron;
 	snn_info const info{ n };
@@ -157,7 +144,7 @@ __global__ void __launch_bounds__( 256 ) slice_fill(
 	for( int j = 0; j < ntiles; j++ )
 	{
 		uint2 const r = rec[(long long)src * ntiles + j];
-		unsigned long long const first = tile_base[j] + r.x;
+		unsigned long long const first = row_base[src] + r.x;
 		__syncwarp();
 		if( lane == 0 ) rec[(long long)src * ntiles + j] = make_uint2( (unsigned)first, r.y );
 		if( r.y == 0 ) continue;

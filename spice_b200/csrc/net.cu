@@ -715,7 +715,10 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 	net.tile_first_host = first;
 	net.tc.ntiles = (int)first.size() - 1;
 	net.tile_first.alloc( first.size() * 4 );
-	CK( cudaMemcpy( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice ) );
+	// on the net's stream (non-blocking: a plain cudaMemcpy from pageable memory may return
+	// before its DMA lands, unordered with the net's kernels)
+	CK( cudaMemcpyAsync( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice, net.stream ) );
+	CK( cudaStreamSynchronize( net.stream ) );
 }
 
 // window_flat's tiling of n neurons into at most about `target` work-balanced tiles (target
@@ -850,7 +853,7 @@ void allocate_buffers( spk_net & net )
 	CK( cudaMemsetAsync( net.err.p, 0, 4, net.stream ) );
 	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
 	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
-	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay );
+	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream );
 	CK( cudaMallocHost( &net.host_count, 16 ) );
 	net.configure();
 }
@@ -872,35 +875,36 @@ void fill_slices( spk_net & net, dbuf const & bases )
 void build_slices( spk_net & net )
 {
 	int const nt = net.tc.ntiles;
-	net.slice_rec.alloc( (size_t)net.n * nt * sizeof( uint2 ) );
-	dbuf totals, bases;
-	totals.alloc( (size_t)nt * 8 );
-	bases.alloc( (size_t)nt * 8 );
-	std::vector<unsigned long long> tot( nt ), base( nt );
-	// vectors per (src, tile) and their per-tile prefix
-	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>(), net.pack );
+	long long const n = net.n;
+	net.slice_rec.alloc( (size_t)n * nt * sizeof( uint2 ) );
+	net.tile_inputs.alloc( (size_t)nt * 4 );
+	CK( cudaMemsetAsync( net.tile_inputs.p, 0, net.tile_inputs.bytes, net.stream ) );
+	dbuf rows, bases;
+	rows.alloc( (size_t)n * 4 );
+	bases.alloc( (size_t)n * 8 );
+	std::vector<unsigned> rv( n );
+	std::vector<unsigned long long> base( n );
+	// vectors per (src, tile), their prefix along each row, and the rows' totals
+	int const blocks = (int)( ( n * 32 + 255 ) / 256 );
+	spk::slice_vectors<<<4 * net.sms, 256, 0, net.stream>>>( (int)n, nt, net.pivots.as<unsigned>(), net.slice_rec.as<uint2>(), net.pack );
 	CK( cudaGetLastError() );
-	spk::slice_offsets<<<nt, 1024, 0, net.stream>>>( (int)net.n, nt, net.slice_rec.as<uint2>(), totals.as<unsigned long long>() );
+	spk::slice_row_offsets<<<blocks, 256, 0, net.stream>>>( (int)n, nt, net.slice_rec.as<uint2>(), rows.as<unsigned>(), net.tile_inputs.as<int>() );
 	CK( cudaGetLastError() );
-	CK( cudaMemcpyAsync( tot.data(), totals.p, (size_t)nt * 8, cudaMemcpyDeviceToHost, net.stream ) );
+	CK( cudaMemcpyAsync( rv.data(), rows.p, (size_t)n * 4, cudaMemcpyDeviceToHost, net.stream ) );
 	CK( cudaStreamSynchronize( net.stream ) );
 	unsigned long long all = 0;
-	for( int j = 0; j < nt; j++ )
+	for( long long s = 0; s < n; s++ )
 	{
-		base[j] = all;
-		all += tot[j];
+		base[s] = all;
+		all += rv[s];
 	}
 	require( all < ( 1ULL << 32 ), "graph too large for 32-bit slice records" );
-	std::vector<int> inputs( nt );
-	for( int j = 0; j < nt; j++ ) inputs[j] = tot[j] > 0;
 	char const * sync = getenv( "SPK_FLAT_SYNC" );
 	net.flat_sync = sync && !strcmp( sync, "1" );
 	net.done_step.alloc( (size_t)nt * sizeof( long long ) );
 	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
-	net.tile_inputs.alloc( (size_t)nt * 4 );
-	CK( cudaMemcpyAsync( net.tile_inputs.p, inputs.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
 	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ) );
-	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)nt * 8, cudaMemcpyHostToDevice, net.stream ) );
+	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)n * 8, cudaMemcpyHostToDevice, net.stream ) );
 	switch( net.model )
 	{
 	case SPK_VOGELS_ABBOTT: fill_slices<spice::vogels_abbott>( net, bases ); break;
@@ -908,7 +912,7 @@ void build_slices( spk_net & net )
 	case SPK_SYNTH: fill_slices<spice::synth>( net, bases ); break;
 	default: break;
 	}
-	CK( cudaStreamSynchronize( net.stream ) ); // totals and bases are freed on return
+	CK( cudaStreamSynchronize( net.stream ) ); // rows and bases are freed on return
 }
 
 void enqueue_pivots( spk_net & net )
@@ -1531,7 +1535,7 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 		CK( cudaMemcpy( &e, net->err.p, 4, cudaMemcpyDeviceToHost ) );
 		if( e & spk::ERR_OVERFLOW )
 		{
-			CK( cudaMemset( net->err.p, 0, 4 ) );
+			CK( cudaMemsetAsync( net->err.p, 0, 4, net->stream ) );
 			throw spk_error( SPK_ERR_CAPACITY, "spike raster buffer too small" );
 		}
 		if( e ) throw spk_error( SPK_ERR_DEVICE, "device error flag " + std::to_string( e ) );
@@ -1733,17 +1737,21 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		// edges first: the pivots and slices are rebuilt from them (which resets the
 		// publication flags), then the state over them
 		dbuf & e = net->edges;
-		if( e.bytes ) CK( cudaMemcpy( e.p, find( 1, e.bytes ), e.bytes, cudaMemcpyHostToDevice ) );
+		// every upload on the net's stream, ahead of the kernels that read it (a plain
+		// cudaMemcpy from pageable memory may return before its DMA lands)
+		if( e.bytes ) CK( cudaMemcpyAsync( e.p, find( 1, e.bytes ), e.bytes, cudaMemcpyHostToDevice, net->stream ) );
 		enqueue_pivots( *net );
 		CK( cudaStreamSynchronize( net->stream ) );
 		for( auto const & x : ckpt_buffers( *net ) )
 		{
 			dbuf & d = *static_cast<dbuf *>( x.second );
 			if( x.first == 1 || d.bytes == 0 ) continue;
-			CK( cudaMemcpy( d.p, find( x.first, d.bytes ), d.bytes, cudaMemcpyHostToDevice ) );
+			CK( cudaMemcpyAsync( d.p, find( x.first, d.bytes ), d.bytes, cudaMemcpyHostToDevice, net->stream ) );
 		}
 		for( auto const & x : ckpt_plastic( *net ) )
-			if( x.second->bytes ) CK( cudaMemcpy( x.second->p, find( x.first, x.second->bytes ), x.second->bytes, cudaMemcpyHostToDevice ) );
+			if( x.second->bytes )
+				CK( cudaMemcpyAsync( x.second->p, find( x.first, x.second->bytes ), x.second->bytes, cudaMemcpyHostToDevice, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
 		net->steps = net->launched = h.steps;
 		net->configure();
 		*out = net.release();

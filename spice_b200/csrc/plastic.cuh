@@ -765,7 +765,7 @@ struct plastic_state
 		       ring_meta.bytes + flush_ring.bytes + flush_cnt.bytes + ring_pot.bytes + tmp.bytes;
 	}
 
-	void allocate( long long n, long long width, int ntiles, int delay )
+	void allocate( long long n, long long width, int ntiles, int delay, cudaStream_t stream )
 	{
 		active = true;
 		W.alloc( (size_t)( n * width ) * 4 );
@@ -781,8 +781,9 @@ struct plastic_state
 		flush_ring.alloc( (size_t)2 * delay * n * 16 );
 		flush_cnt.alloc( (size_t)2 * delay * ntiles * 4 );
 		ring_pot.alloc( (size_t)2 * delay * ntiles * 4 );
-		cudaMemset( flush_cnt.p, 0, flush_cnt.bytes );
-		cudaMemset( ring_pot.p, 0, ring_pot.bytes );
+		// on the net's stream, ahead of the kernels that read them
+		cudaMemsetAsync( flush_cnt.p, 0, flush_cnt.bytes, stream );
+		cudaMemsetAsync( ring_pot.p, 0, ring_pot.bytes, stream );
 	}
 
 	plastic_params params() const
