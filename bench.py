@@ -61,13 +61,17 @@ def parse():
 
 
 def dist_init(n):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / MASTER_*): NCCL with GPUs, gloo
+    without (the CPU tests of the multi-rank plumbing)."""
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if world > 1:
-        import torch.distributed as dist
         import datetime
 
-        backend = "nccl"
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return rank, world
 
@@ -85,7 +89,8 @@ def max_over_ranks(x, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
