@@ -603,6 +603,8 @@ struct smem_state
 // before staging a step, a tile waits until every source tile has published the step
 // `delay` earlier. With the pipeline checking five steps ahead that is a step before its
 // own current one (delay >= 6), so the slowest tile never waits and every wait ends.
+// Shorter delays run such launches on the synchronous path only (flat_sync): a step is
+// staged after every tile has published the steps it reads, all before the current one.
 template <typename Model>
 __device__ __forceinline__ void window_flat_body( net_params const & p, int const tile, int L, float dt, int smem_bytes )
 {

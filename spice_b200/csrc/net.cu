@@ -356,7 +356,7 @@ struct spk_net
 				CK( cudaDeviceGetAttribute( &coop, cudaDevAttrCooperativeLaunch, device ) );
 				CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_flat<Model>, tc.threads, flat_smem ) );
 				char const * pers = getenv( "SPK_PERSIST" );
-				persistent = coop && delay >= 6 && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
+				persistent = coop && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
 				return;
 			}
 		// the limit is per kernel, shared by every net: set it to all a CTA can have, so a
@@ -517,6 +517,9 @@ struct spk_net
 		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
 		{
 			auto p = params();
+			// the step pipeline looks five steps ahead, which needs delay >= 6; shorter delays
+			// run every step on the synchronous path (each step waits for the steps it reads)
+			if( delay < 6 ) p.flat_sync = 1;
 			int smem = flat_smem;
 			float d = dt;
 			void * args[] = { &p, &L, &d, &smem };

@@ -282,6 +282,8 @@ def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage, deg):
     ("synth", [300_000], [(0, 0, 16 / 300_000)], 6, 200),               # delay 6: checks the step before
     ("synth", [400_000], [(0, 0, 16 / 400_000)], 8, 120),               # > 1024 arrivals a step: pipeline restarts
     ("vogels_abbott", [4000], [(0, 0, 0.02)], 8, 500),
+    ("vogels_abbott", [5000], [(0, 0, 0.02)], 1, 400),                 # delay 1: synchronous path, waits every step
+    ("brunel", [8000, 8000], [(0, 1, 0.1), (1, 1, 0.1)], 3, 300),       # delay 3
 ])
 def test_persistent_run_matches_windows(model, pops, conns, delay, steps):
     """run() as one cooperative launch in which tiles wait for each other's published
