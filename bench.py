@@ -43,15 +43,16 @@ def parse():
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--syn", type=float, default=1e9,
                     help="total synapses of the Brunel net (the benchmark is 1e9; smaller sizes serve profiling)")
-    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched", "serving"],
+    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched", "serving", "va", "brunel_plus"],
                     help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop; "
-                         "serving: Poisson job arrivals, server vs plain per-job loop")
+                         "serving: Poisson job arrivals, server vs plain per-job loop; va: Vogels-Abbott 4000+1000 "
+                         "at delay 1; brunel_plus: Brunel with STDP at 5e8 synapses")
     ap.add_argument("--duration", type=float, default=8.0, help="serving: seconds of job arrivals")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: job arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
     ap.add_argument("--quantum", type=int, default=600, help="serving: steps per tick")
     ap.add_argument("--nets", type=int, default=256, help="batched: number of nets")
-    ap.add_argument("--bio", type=float, default=1.0, help="batched: biological seconds per net")
+    ap.add_argument("--bio", type=float, default=1.0, help="batched, va, brunel_plus: biological seconds per net")
     args = ap.parse_args()
     if args.syn != 1e9:
         # samples/main.cpp:1283,1395: N = sqrt(syn / 0.05), two populations of N / 2
@@ -536,6 +537,76 @@ def run_serving(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_model_workload(args, rank, world):
+    """Vogels-Abbott (4,000 + 1,000 neurons, p = 0.02, delay 1; the reference's CPU-runnable
+    case) or Brunel+ (N = 100,000, 5e8 synapses, delay 15, lazy STDP): wall/bio through
+    spk_net_run, the raster through spk_net_run_record (e2e), and the reference's cpu::snn on
+    one core (the whole second for VA; a small Brunel+ net, since its CPU STDP sweep touches
+    every synapse every step)."""
+    import torch
+
+    from spice_b200 import Layout, Snn
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    if args.workload == "va":
+        model, pops, conns, delay, syn = "vogels_abbott", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02
+    else:
+        model, pops, conns, delay, syn = "brunel_with_plasticity", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8
+    steps = int(round(args.bio / DT))
+    t0 = time.perf_counter()
+    net = Snn(model, Layout(pops, conns), dt=DT, delay=delay, seed=1 + rank, graph_seed=1337 + rank, device=dev)
+    net.sync()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+    for _ in range(max(3, args.warmup)):
+        net.run(max(delay, 15))
+    net.sync()
+    barrier(world)
+    clocks = Clocks(dev)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    net.run(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    t = time.perf_counter()
+    counts, ids = net.run_record(steps, cap=sum(pops) * steps // 20 + 1024)
+    e2e = max_over_ranks(time.perf_counter() - t, world)
+    info = net.info()
+    net.close()
+    line = {"metric": f"wall/bio time ratio, {model}", "value": ms / 1e3 / (steps * DT), "unit": "wall_s/bio_s",
+            "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "neurons": sum(pops), "synapses": syn, "delay": delay, "dt": DT,
+                       "bio_s": steps * DT, "sim_steps": steps, "setup_s": setup_s, "persistent": bool(info.persistent),
+                       "tiles": info.num_tiles, "spikes_per_step": float(np.mean(counts))},
+            "e2e": {"value": e2e / (steps * DT), "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int((counts.nbytes + ids.nbytes) / 1)},
+            "gpu_launches": info.kernel_launches, "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        fast = oracle.have_reference(fast=True)
+        cpu_pops = pops if args.workload == "va" else [2000, 2000]
+        cpu_steps = steps if args.workload == "va" else 200
+        mk = (lambda: oracle.ReferenceNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, fast=True)) if fast else \
+             (lambda: oracle.OracleNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, graph="reference", graph_seed=1337))
+        cpu = mk()
+        t = time.perf_counter()
+        for _ in range(cpu_steps):
+            cpu.step()
+        wall = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": wall / (cpu_steps * DT), "unit": "wall_s/bio_s", "cores": 1,
+                                "kind": "reference" if fast else "port",
+                                "sample": f"{model} N={sum(cpu_pops)}, {cpu_steps} steps, single thread"
+                                          + ("" if args.workload == "va" else " (small N: the CPU STDP sweep is eager over all synapses)")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
@@ -546,6 +617,8 @@ def main():
             run_batched(args, rank, world)
         elif args.workload == "serving":
             run_serving(args, rank, world)
+        elif args.workload in ("va", "brunel_plus"):
+            run_model_workload(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:
