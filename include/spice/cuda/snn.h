@@ -150,7 +150,39 @@ public:
 	}
 	spk_net * handle() const { return _net; }
 
+	// everything the net needs to continue bit for bit (edges, state, spikes in flight,
+	// clock, lazy-STDP state); restore() makes a net continuing from it
+	std::vector<unsigned char> checkpoint() const
+	{
+		std::uint64_t size = 0;
+		check( spk_net_checkpoint( _net, nullptr, 0, &size ) );
+		std::vector<unsigned char> buf( size );
+		check( spk_net_checkpoint( _net, buf.data(), buf.size(), &size ) );
+		return buf;
+	}
+	static snn restore( std::vector<unsigned char> const & buf, int device = 0 )
+	{
+		spk_net * h = nullptr;
+		check( spk_net_restore( &h, buf.data(), buf.size(), device ) );
+		spk_net_info i{};
+		int const st = spk_net_get_info( h, &i );
+		if( st != SPK_OK || i.model != model_id<Model>::value )
+		{
+			spk_net_destroy( h );
+			throw std::invalid_argument( "the checkpoint holds another model" );
+		}
+		return snn( h );
+	}
+	snn( snn && other ) noexcept
+	    : _net( std::exchange( other._net, nullptr ) )
+	{
+	}
+
 private:
+	explicit snn( spk_net * h )
+	    : _net( h )
+	{
+	}
 	spk_net * _net = nullptr;
 
 	static void flatten_to_pops( util::layout const & l, std::vector<std::uint64_t> & pops, std::vector<int> & src, std::vector<int> & dst, std::vector<float> & p )

@@ -1,5 +1,6 @@
 // C++17 surface test (restates spice_test/cuda/snn.d.cpp:72-139 against the C++ wrapper):
 // construction, conversion constructor, stepping, export. Exit code 0 = pass.
+#include <spice/cuda/batch.h>
 #include <spice/cuda/snn.h>
 
 #include <cstdio>
@@ -47,6 +48,43 @@ int main()
 		EXPECT( s.size() == d.num_synapses() );
 		std::vector<int> out;
 		d.step( &out );
+	}
+	{ // checkpoint / restore: the restored net continues bit for bit
+		cuda::snn<brunel> a( util::layout( { 2000, 2000 }, { { 0, 1, 0.1f }, { 1, 1, 0.1f } } ), 0.0001f, 15 );
+		a.run( 123 );
+		auto b = cuda::snn<brunel>::restore( a.checkpoint() );
+		std::vector<int> sa, sb;
+		for( int i = 0; i < 100; i++ )
+		{
+			a.step( &sa );
+			b.step( &sb );
+			EXPECT( sa == sb );
+		}
+		EXPECT( a.neurons() == b.neurons() );
+		bool thrown = false;
+		try
+		{
+			cuda::snn<vogels_abbott>::restore( a.checkpoint() );
+		}
+		catch( std::invalid_argument const & )
+		{
+			thrown = true;
+		}
+		EXPECT( thrown );
+	}
+	{ // a batch steps its nets as they step alone; a server job ends with the same state
+		util::layout const l( { 1500, 1500 }, { { 0, 1, 0.1f }, { 1, 1, 0.1f } } );
+		cuda::snn<brunel> alone( l, 0.0001f, 15, 5 ), in_batch( l, 0.0001f, 15, 5 );
+		cuda::batch b;
+		b.add( in_batch );
+		b.run( 200 );
+		alone.run( 200 );
+		EXPECT( alone.neurons() == in_batch.neurons() );
+		cuda::server srv( 1ull << 32, 100 );
+		auto const job = srv.submit<brunel>( l, 250, 0.0001f, 15, 5 );
+		srv.wait( job, 60.0 );
+		EXPECT( srv.info( job ).state == SPK_JOB_DONE && srv.info( job ).steps_done == 250 );
+		EXPECT( srv.stats().done == 1 );
 	}
 	{ // errors come back as the reference's exception types
 		bool thrown = false;
