@@ -776,26 +776,21 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 					int const eb = m_e[sb & 7];
 					for( int g = pt; g < eb; g += npt ) cp_async8( e2 + g, p.slice_rec + (long long)e2[g].x * p.ntiles + tile );
 				}
-				// spike ids of step j + 3 (its per-source-tile counts are scanned)
+				// spike ids of step j + 3 (its per-source-tile counts are scanned), one source
+				// tile per thread
 				int const sc = j + 3;
 				if( sc >= kb && sc < L && !m_big[sc & 7] )
 				{
 					int const * pc = pcnt + ( sc & 3 ) * FLAT_PC;
 					int2 * e3 = ent + ( sc & 3 ) * FLAT_STEP_CAP;
-					int const ec = m_e[sc & 7];
 					long long const slot = ( ( t0 + sc - p.delay ) % p.ring ) * (long long)p.n;
-					for( int g = pt; g < ec; g += npt )
+					// source tile i's spikes are ring_ids[slot + tile_first[i] + r], r < its count
+					for( int i = pt; i < p.ntiles; i += npt )
 					{
-						int lo = 0, hi = p.ntiles; // last source tile i with pc[i] <= g
-						while( hi - lo > 1 )
-						{
-							int const mid = ( lo + hi ) >> 1;
-							if( pc[mid] <= g )
-								lo = mid;
-							else
-								hi = mid;
-						}
-						cp_async4( &e3[g].x, p.ring_ids + slot + __ldg( p.tile_first + lo ) + ( g - pc[lo] ) );
+						int const g0 = pc[i], g1 = pc[i + 1];
+						if( g0 == g1 ) continue;
+						int const * ids = p.ring_ids + slot + __ldg( p.tile_first + i );
+						for( int r = 0; r < g1 - g0; r++ ) cp_async4( &e3[g0 + r].x, ids + r );
 					}
 				}
 				// per-source-tile spike counts of step j + 4 (none before `delay`): every
@@ -818,9 +813,10 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 							pc[i] = 0;
 					}
 				}
-				// publication of the spikes step j + 5 reads, checked while the copies above
-				// are in flight (a step before its own one for delay >= 6: no wait in practice)
-				if( j + 5 >= kb && j + 5 < L && j + 5 + t0 >= p.delay )
+				// publication of the spikes step j + 5 reads (a step before its own one for
+				// delay >= 6: no wait in practice): checked here in the prologue, by the
+				// publisher warp during the pipelined steps
+				if( all && j + 5 >= kb && j + 5 < L && j + 5 + t0 >= p.delay )
 					for( int i = pt; i < p.ntiles; i += npt ) wait_published( p, i, t0 + j + 5 - p.delay );
 				cp_async_commit();
 				cp_async_wait_all();
@@ -944,8 +940,11 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 					else if( warp == nw - 1 )
 					{
 						// the publisher warp: step k - 1's spikes to the ring, fenced, then its
-						// flag (the fence waits for the stores; no producer waits on it)
+						// flag (the fence waits for the stores; no producer waits on it); then
+						// the publication of the spikes step k + 5 reads, for the producers'
+						// next step (relaxed reads of every flag, one acquire fence)
 						if( k > kb ) compact( k - 1 );
+						if( k + 5 < L && t0 + k + 5 >= p.delay ) warp_wait_all_published( p, t0 + k + 5 - p.delay );
 					}
 					else
 						produce( k, tid - ncons, nt - ncons - 32, false );
