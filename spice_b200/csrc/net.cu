@@ -1095,7 +1095,12 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	net->dt = dt;
 	net->delay = delay;
 	net->seed = seed;
-	CK( cudaStreamCreateWithFlags( &net->stream, cudaStreamNonBlocking ) );
+	device_guard g( device ); // the stream belongs to the net's device
+	// a net's own work (building it, its windows, exports) at the highest stream priority:
+	// beside the long shared launches of a batch its CTAs start as soon as an SM frees up
+	int least = 0, greatest = 0;
+	CK( cudaDeviceGetStreamPriorityRange( &least, &greatest ) );
+	CK( cudaStreamCreateWithPriority( &net->stream, cudaStreamNonBlocking, greatest ) );
 	return net.release();
 }
 } // namespace
@@ -1913,7 +1918,9 @@ int spk_batch_create( spk_batch ** out, int device )
 		b->device = device;
 		for( auto & g : b->groups )
 		{
-			CK( cudaStreamCreateWithFlags( &g.stream, cudaStreamNonBlocking ) );
+			int least = 0, greatest = 0;
+			CK( cudaDeviceGetStreamPriorityRange( &least, &greatest ) );
+			CK( cudaStreamCreateWithPriority( &g.stream, cudaStreamNonBlocking, least ) );
 			CK( cudaEventCreateWithFlags( &g.ev, cudaEventDisableTiming ) );
 		}
 		*out = b.release();
