@@ -485,3 +485,47 @@ def test_checkpoint_restore_continues_bit_for_bit(model, pops, conns, delay, fir
     for x, y in zip(a.synapses(), b.synapses()):
         assert bits_equal(x, y)
     assert np.array_equal(a.adj()[0], b.adj()[0])
+
+
+# ----------------------------------------------------------------------- edge cases
+@pytest.mark.parametrize("model,pops,conns,delay,steps", [
+    ("brunel", [500, 500], [(0, 1, 0.0), (1, 1, 0.0)], 15, 200),      # no synapses at all (width 0)
+    ("vogels_abbott", [1001], [(0, 0, 0.02)], 1, 300),               # size not a multiple of 32
+    ("brunel", [1], [], 3, 60),                                       # one neuron, no connections
+    ("synth", [3000], [(0, 0, 0.01)], 100, 260),                      # delay above the 64-step window
+    ("brunel_with_plasticity", [300, 301], [(0, 1, 0.1), (1, 1, 0.1)], 63, 200),  # the plastic delay limit
+])
+def test_edge_cases_step_by_step(model, pops, conns, delay, steps):
+    """Empty, odd-sized and single-neuron nets, and delays at and beyond the window limits,
+    against the oracle, spike by spike."""
+    run_parity(model, pops, conns, delay, steps, seed=3, check_w=model == "brunel_with_plasticity")
+
+
+@pytest.mark.parametrize("model,pops,conns,delay,steps", [
+    ("synth", [3000], [(0, 0, 0.01)], 100, 450),                      # long persistent run, delay 100
+    ("brunel", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], 64, 400),    # delay = window limit
+    ("vogels_abbott", [1001], [(0, 0, 0.02)], 7, 333),                # delay 7: the synchronous path in one launch
+])
+def test_edge_cases_bulk_runs(model, pops, conns, delay, steps):
+    """The same through run() (one persistent launch or graphs of windows) against the
+    oracle's final state, then step-by-step output after it."""
+    net = Snn(model, Layout(pops, conns), delay=delay, seed=4, graph_seed=4)
+    edges, width = net.adj()
+    ref = oracle.OracleNet(model, pops, conns, delay=delay, seed=4, edges=edges, width=width)
+    net.run(steps)
+    for _ in range(steps):
+        ref.step()
+    check_neurons(model, net.neurons(), ref.neurons())
+    for i in range(3):
+        assert np.array_equal(net.step(out=True), ref.step()), i
+
+
+def test_zero_steps_and_small_output_buffers():
+    net = Snn("brunel", Layout([2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15, seed=1)
+    net.run(0)
+    counts, ids = net.run_record(0)
+    assert len(counts) == 0 and len(ids) == 0 and net.info().steps == 0
+    net.run(100)
+    with pytest.raises(spice_b200.CapacityError):
+        net.run_record(50, cap=1)  # Poisson neurons alone fire more than one spike in 50 steps
+    assert net.info().steps == 150  # the state advanced; nothing was copied
