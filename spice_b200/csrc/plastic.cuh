@@ -386,8 +386,32 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 				{
 					int const mc = min( PL_CHUNK, m - c0 );
 					if( tid < mc ) s_src[tid] = sb[c0 + tid].src;
-					for( int x = warp; x < mc; x += nw )
+					// each warp's spikes of the chunk (x = warp, warp + nw, ...): the first target
+					// and weight of every spike's row slice loaded before any is processed, so
+					// the rows' global loads overlap instead of running one after another
+					constexpr int PL_AHEAD = PL_CHUNK / 4; // spikes per warp, 4 warps at least
+					int pd[PL_AHEAD];
+					float pw[PL_AHEAD];
+#pragma unroll
+					for( int u = 0; u < PL_AHEAD; u++ )
 					{
+						int const x = warp + u * nw;
+						pd[u] = -1;
+						pw[u] = 0.0f;
+						if( x < mc )
+						{
+							stage_e const e = sb[c0 + x];
+							int const j = e.lo + lane;
+							if( j < e.hi )
+							{
+								pd[u] = __ldg( p.edges + (long long)e.src * p.width + j );
+								pw[u] = q.W[(long long)e.src * p.width + j];
+							}
+						}
+					}
+					// spike x of the chunk into its weight column; (d1st, w1st) = its first slice
+					// element if loaded ahead (ahead1st)
+					auto arrive = [&]( int x, bool ahead1st, int d1st, float w1st ) {
 						stage_e const e = sb[c0 + x];
 						int const rf_off = e.meta & 0xff;
 						bool const replay = rf_off > 0 && Syn::plastic_src( e.src, info );
@@ -405,14 +429,15 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 						unsigned long long const wm = rf_off >= 64 ? ~0ull : ( ( 1ull << rf_off ) - 1 );
 						for( int j = e.lo + lane; j < e.hi; j += 32 )
 						{
-							int const d = __ldg( row + j );
+							bool const ahead = ahead1st && j == e.lo + lane;
+							int const d = ahead ? d1st : __ldg( row + j );
 							int const local = d - d0;
 							if( (unsigned)local >= (unsigned)span )
 							{
 								atomicOr( p.err, ERR_BAD_TARGET );
 								continue;
 							}
-							float w = wrow[j];
+							float w = ahead ? w1st : wrow[j];
 							if( replay && Syn::plastic_dst( d, info ) )
 							{
 								unsigned long long const hb = sh_hist[local] & wm;
@@ -427,7 +452,12 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 							atomicOr( mask + local, bit );
 						}
 						if( replay ) __syncwarp();
-					}
+					};
+#pragma unroll
+					for( int u = 0; u < PL_AHEAD; u++ )
+						if( warp + u * nw < mc ) arrive( warp + u * nw, true, pd[u], pw[u] );
+					// narrow CTAs (fewer than four warps): the rest without loads ahead
+					for( int x = warp + PL_AHEAD * nw; x < mc; x += nw ) arrive( x, false, 0, 0.0f );
 					__syncthreads();
 					// every target adds its inputs in ascending source order
 #pragma unroll
