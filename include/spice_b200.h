@@ -187,6 +187,10 @@ int spk_net_stream( spk_net * net, void ** out_stream );
 /* Wait for all queued work; reports device-side errors. */
 int spk_net_sync( spk_net * net );
 
+/* Queued steps launched; *out_idle = 1 if the net's stream has finished all its work
+ * (without waiting; device-side errors are reported by spk_net_sync). */
+int spk_net_idle( spk_net * net, int * out_idle );
+
 int spk_net_get_info( spk_net * net, spk_net_info * out );
 
 /* snn::adj() (spice/snn.h:31): the ELL edges (num_neurons * width int32). */
@@ -239,8 +243,8 @@ int spk_batch_run_nets( spk_batch * batch, int count, spk_net * const * nets, ui
 int spk_batch_destroy( spk_batch * batch );
 
 /* ---- serving: jobs admitted against a device-memory budget, continuously batched ----
- * A server owns two worker threads (one builds admitted jobs' nets, one steps the batch)
- * and one batch on `device`. Submitted jobs queue in
+ * A server owns builder threads (they build admitted jobs' nets), a ticker thread (it
+ * steps the batch) and one batch on `device`. Submitted jobs queue in
  * arrival order; the head is admitted when its estimated device memory
  * (spk_net_estimate_bytes) fits the budget beside the running jobs, and its net is built
  * with a tile count sized to its share of the load. Every tick advances each running job

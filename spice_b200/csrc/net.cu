@@ -112,6 +112,90 @@ struct dbuf
 	}
 };
 
+// 16-byte pinned host slots for the nets' small device-to-host reads, carved from slabs
+// allocated once: a page-locked allocation synchronises the whole device, which a net
+// built beside a running batch should not do
+class pinned_slots
+{
+public:
+	static unsigned * get()
+	{
+		std::lock_guard<std::mutex> lk( mu() );
+		auto & f = free_list();
+		if( f.empty() )
+		{
+			void * slab = nullptr;
+			CK( cudaMallocHost( &slab, SLAB ) );
+			for( size_t o = 0; o < SLAB; o += 16 ) f.push_back( reinterpret_cast<unsigned *>( static_cast<char *>( slab ) + o ) );
+		}
+		unsigned * q = f.back();
+		f.pop_back();
+		return q;
+	}
+	static void put( unsigned * q )
+	{
+		if( !q ) return;
+		std::lock_guard<std::mutex> lk( mu() );
+		free_list().push_back( q );
+	}
+
+private:
+	static constexpr size_t SLAB = 64 * 1024;
+	static std::mutex & mu()
+	{
+		static std::mutex m;
+		return m;
+	}
+	static std::vector<unsigned *> & free_list()
+	{
+		static std::vector<unsigned *> f;
+		return f;
+	}
+};
+
+// Scratch device memory ordered on a stream, from a per-device pool that keeps its memory:
+// unlike cudaFree, releasing it does not wait for the whole device, so a net built beside
+// a running batch does not stall on the batch's launches.
+cudaMemPool_t scratch_pool( int device )
+{
+	static std::mutex m;
+	static std::vector<cudaMemPool_t> pools;
+	std::lock_guard<std::mutex> lk( m );
+	if( (int)pools.size() <= device ) pools.resize( device + 1, nullptr );
+	if( !pools[device] )
+	{
+		cudaMemPoolProps props{};
+		props.allocType = cudaMemAllocationTypePinned;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id = device;
+		CK( cudaMemPoolCreate( &pools[device], &props ) );
+		unsigned long long keep = ~0ull;
+		CK( cudaMemPoolSetAttribute( pools[device], cudaMemPoolAttrReleaseThreshold, &keep ) );
+	}
+	return pools[device];
+}
+struct sbuf
+{
+	void * p = nullptr;
+	cudaStream_t s = nullptr;
+	sbuf( size_t b, cudaStream_t st, int device )
+	    : s( st )
+	{
+		if( b ) CK( cudaMallocFromPoolAsync( &p, b, scratch_pool( device ), s ) );
+	}
+	sbuf( sbuf const & ) = delete;
+	sbuf & operator=( sbuf const & ) = delete;
+	~sbuf()
+	{
+		if( p ) cudaFreeAsync( p, s );
+	}
+	template <typename T>
+	T * as() const
+	{
+		return static_cast<T *>( p );
+	}
+};
+
 // restores the caller's current device on scope exit
 struct device_guard
 {
@@ -228,7 +312,7 @@ struct spk_net
 	unsigned long long launched = 0; // steps launched
 	unsigned long long kernel_launches = 0; // simulation kernel launches (graph replays counted per window)
 	int ring_slots = 0;                      // steps the spike ring holds (2 delay; more for recording runs)
-	unsigned * host_count = nullptr; // pinned
+	unsigned * host_count = nullptr; // pinned (a pinned_slots slot)
 
 	cudaGraphExec_t graph = nullptr;
 	int graph_windows = 0, graph_len = 0;
@@ -249,7 +333,7 @@ struct spk_net
 	~spk_net()
 	{
 		if( graph ) cudaGraphExecDestroy( graph );
-		if( host_count ) cudaFreeHost( host_count );
+		pinned_slots::put( host_count );
 		if( stream ) cudaStreamDestroy( stream );
 	}
 
@@ -857,12 +941,12 @@ void allocate_buffers( spk_net & net )
 	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
 	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
 	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream );
-	CK( cudaMallocHost( &net.host_count, 16 ) );
+	if( !net.host_count ) net.host_count = pinned_slots::get();
 	net.configure();
 }
 
 template <typename Model>
-void fill_slices( spk_net & net, dbuf const & bases )
+void fill_slices( spk_net & net, sbuf const & bases )
 {
 	if constexpr( Model::neuron::input_classes > 0 )
 	{
@@ -882,9 +966,7 @@ void build_slices( spk_net & net )
 	net.slice_rec.alloc( (size_t)n * nt * sizeof( uint2 ) );
 	net.tile_inputs.alloc( (size_t)nt * 4 );
 	CK( cudaMemsetAsync( net.tile_inputs.p, 0, net.tile_inputs.bytes, net.stream ) );
-	dbuf rows, bases;
-	rows.alloc( (size_t)n * 4 );
-	bases.alloc( (size_t)n * 8 );
+	sbuf rows( (size_t)n * 4, net.stream, net.device ), bases( (size_t)n * 8, net.stream, net.device );
 	std::vector<unsigned> rv( n );
 	std::vector<unsigned long long> base( n );
 	// vectors per (src, tile), their prefix along each row, and the rows' totals
@@ -1560,6 +1642,18 @@ int spk_net_stream( spk_net * net, void ** out_stream )
 		device_guard g( net->device );
 		net->flush();
 		*out_stream = net->stream;
+	} );
+}
+
+int spk_net_idle( spk_net * net, int * out_idle )
+{
+	return guarded( [&] {
+		require( net != nullptr && out_idle != nullptr, "null argument" );
+		device_guard g( net->device );
+		net->flush();
+		cudaError_t const e = cudaStreamQuery( net->stream );
+		if( e != cudaErrorNotReady ) CK( e );
+		*out_idle = e == cudaSuccess ? 1 : 0;
 	} );
 }
 

@@ -2,11 +2,11 @@
 // budget, stepped together by continuous batching.
 //
 // The reference has no server; a workload of many nets is a host loop that builds and steps
-// one net after another (spice_bench/paper_plots.cpp:184-231). Here two threads per server
-// own the GPU side:
-//   builder  admits queued jobs in arrival order while their estimated device memory fits
+// one net after another (spice_bench/paper_plots.cpp:184-231). Here a few builder threads
+// and one ticker thread per server own the GPU side:
+//   builders admit queued jobs in arrival order while their estimated device memory fits
 //            the budget (a job larger than the whole budget is refused at submission) and
-//            builds each admitted job's net, with a tile count sized to its share of the
+//            build each admitted job's net, with a tile count sized to its share of the
 //            load, while the ticker steps the others;
 //   ticker   each tick advances every running job by up to `quantum` steps in one batch
 //            run (jobs built since the last tick join it: continuous batching), then
@@ -36,6 +36,10 @@ void spk_set_last_error( std::string const & msg );
 
 namespace
 {
+// builder threads (one: concurrent builds measured slower, their device-wide
+// synchronisations -- allocations, frees -- queue behind each other and the ticker's work)
+constexpr int BUILDERS = 1;
+
 int fail( int code, std::string const & msg )
 {
 	spk_set_last_error( msg );
@@ -64,6 +68,8 @@ struct job
 	bool cancel = false;
 	spk_net * net = nullptr;
 	double work = 0;                           // expected cost per step (tiling share)
+	bool own = false;                          // steps on its own stream, not in the shared launches (Brunel+)
+	uint64_t inflight = 0;                     // own-stream steps launched, not yet seen finished
 	std::vector<std::vector<uint32_t>> result; // final neuron attributes (4-byte words)
 
 	spk_layout_desc desc() const
@@ -94,7 +100,8 @@ struct server
 	uint64_t in_use = 0, peak = 0, ticks = 0;
 	double build_s = 0, tick_s = 0;
 	int inject = 0;
-	std::thread builder, ticker;
+	std::vector<std::thread> builders; // BUILDERS threads admit and build concurrently
+	std::thread ticker;
 
 	double now() const { return std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count(); }
 
@@ -194,10 +201,18 @@ struct server
 			lk.unlock();
 			std::vector<std::pair<job *, std::string>> rejected;
 			for( auto * j : joining )
-				if( spk_batch_add( batch, j->net ) == SPK_OK )
+			{
+				spk_net_info info{};
+				if( spk_net_get_info( j->net, &info ) == SPK_OK && spk_batch_add( batch, j->net ) == SPK_OK )
+				{
+					// nets outside the shared launches run on their own streams, each at its
+					// own pace: the ticks of the shared launches do not wait for them
+					j->own = info.model == SPK_BRUNEL_PLUS || info.slice_pack == 0;
 					running_t.push_back( j );
+				}
 				else
 					rejected.push_back( { j, spk_last_error() } );
+			}
 			for( auto & r : rejected )
 			{
 				spk_net_destroy( r.first->net );
@@ -216,21 +231,63 @@ struct server
 				tick_wake.wait_for( lk, std::chrono::milliseconds( 20 ) );
 				continue;
 			}
-			// one tick: every running job up to `quantum` steps
+			// one tick: every job of the shared launches up to `quantum` steps, synchronised;
+			// own-stream jobs: a finished quantum is counted and the next one launched
 			std::vector<spk_net *> nets;
 			std::vector<uint64_t> counts;
-			std::vector<job *> ticked;
+			std::vector<job *> ticked, owns;
 			for( auto * j : running_t )
-				if( !j->cancel && j->done < j->nsteps )
+			{
+				if( j->own )
+					owns.push_back( j );
+				else if( !j->cancel && j->done < j->nsteps )
 				{
 					nets.push_back( j->net );
 					counts.push_back( std::min( quantum, j->nsteps - j->done ) );
 					ticked.push_back( j );
 				}
+			}
 			lk.unlock();
 			double const tt = now();
 			std::vector<int> status( ticked.size(), SPK_OK );
 			std::vector<std::string> msgs( ticked.size() );
+			std::vector<int> own_status( owns.size(), SPK_OK );
+			std::vector<std::string> own_msgs( owns.size() );
+			std::vector<uint64_t> own_done( owns.size(), 0 ), own_launch( owns.size(), 0 );
+			bool own_busy = false;
+			for( size_t i = 0; i < owns.size(); i++ )
+			{
+				job & j = *owns[i];
+				int idle = 0;
+				int r = spk_net_idle( j.net, &idle );
+				if( r == SPK_OK && idle && j.inflight ) r = spk_net_sync( j.net ); // its quantum ended: errors?
+				if( r != SPK_OK )
+				{
+					own_status[i] = r;
+					own_msgs[i] = spk_last_error();
+					continue;
+				}
+				if( !idle )
+				{
+					own_busy = true;
+					continue;
+				}
+				own_done[i] = j.inflight;
+				uint64_t const left = j.nsteps - j.done - j.inflight;
+				if( !j.cancel && left > 0 )
+				{
+					own_launch[i] = std::min( quantum, left );
+					r = spk_net_run( j.net, own_launch[i] );
+					if( r != SPK_OK )
+					{
+						own_status[i] = r;
+						own_msgs[i] = spk_last_error();
+						own_launch[i] = 0;
+					}
+					else
+						own_busy = true;
+				}
+			}
 			int rc = nets.empty() ? SPK_OK : spk_batch_run_nets( batch, (int)nets.size(), nets.data(), counts.data() );
 			std::string const run_msg = rc != SPK_OK ? spk_last_error() : "";
 			for( size_t i = 0; i < ticked.size(); i++ )
@@ -243,6 +300,18 @@ struct server
 			tick_s += now() - tt;
 			for( size_t i = 0; i < ticked.size(); i++ )
 				if( status[i] == SPK_OK ) ticked[i]->done += counts[i];
+			for( size_t i = 0; i < owns.size(); i++ )
+			{
+				owns[i]->done += own_done[i];
+				owns[i]->inflight = own_launch[i] ? own_launch[i] : ( own_done[i] ? 0 : owns[i]->inflight );
+			}
+			// the same outcome lists for both kinds of jobs
+			for( size_t i = 0; i < owns.size(); i++ )
+			{
+				ticked.push_back( owns[i] );
+				status.push_back( own_status[i] );
+				msgs.push_back( own_msgs[i] );
+			}
 			// retire
 			double const te = now();
 			std::vector<std::pair<job *, int>> leaving; // (job, final state)
@@ -256,6 +325,7 @@ struct server
 				int state = -1;
 				if( st != SPK_OK ) state = SPK_JOB_FAILED;
 				else if( j.done >= j.nsteps ) state = SPK_JOB_DONE;
+				else if( j.own && j.inflight ) state = -1; // its quantum still runs
 				else if( j.cancel ) state = SPK_JOB_CANCELLED;
 				else if( j.timeout_s > 0 && te - j.t_submit > j.timeout_s ) state = SPK_JOB_TIMEOUT;
 				if( state < 0 )
@@ -309,6 +379,8 @@ struct server
 				finish( j, leaving[i].second, errs[i], emsgs[i] );
 			}
 			if( !leaving.empty() ) wake.notify_all(); // budget freed
+			// only own-stream jobs running, all busy: poll again shortly, not in a spin
+			if( nets.empty() && own_busy && leaving.empty() ) tick_wake.wait_for( lk, std::chrono::microseconds( 200 ) );
 		}
 	}
 };
@@ -332,7 +404,7 @@ int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uin
 		return fail( SPK_ERR_INVALID, "invalid device" );
 	int const rc = spk_batch_create( &s->batch, device );
 	if( rc != SPK_OK ) return rc;
-	s->builder = std::thread( [p = s.get()] { p->build_loop(); } );
+	for( int b = 0; b < BUILDERS; b++ ) s->builders.emplace_back( [p = s.get()] { p->build_loop(); } );
 	s->ticker = std::thread( [p = s.get()] { p->tick_loop(); } );
 	*out = s.release();
 	return SPK_OK;
@@ -521,7 +593,8 @@ int spk_server_destroy( spk_server * s )
 		s->wake.notify_all();
 		s->tick_wake.notify_all();
 	}
-	if( s->builder.joinable() ) s->builder.join();
+	for( auto & b : s->builders )
+		if( b.joinable() ) b.join();
 	if( s->ticker.joinable() ) s->ticker.join();
 	for( auto * j : s->ready )
 		spk_net_destroy( j->net );
