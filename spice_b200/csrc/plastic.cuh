@@ -386,32 +386,41 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 				{
 					int const mc = min( PL_CHUNK, m - c0 );
 					if( tid < mc ) s_src[tid] = sb[c0 + tid].src;
-					// each warp's spikes of the chunk (x = warp, warp + nw, ...): the first target
-					// and weight of every spike's row slice loaded before any is processed, so
-					// the rows' global loads overlap instead of running one after another
+					// each warp's spikes of the chunk (x = warp, warp + nw, ...): the first two
+					// targets and weights per lane of every spike's row slice loaded before any is
+					// processed, so the rows' global loads overlap instead of running one after
+					// another
 					constexpr int PL_AHEAD = PL_CHUNK / 4; // spikes per warp, 4 warps at least
-					int pd[PL_AHEAD];
-					float pw[PL_AHEAD];
+					int pd[PL_AHEAD][2];
+					float pw[PL_AHEAD][2];
 #pragma unroll
 					for( int u = 0; u < PL_AHEAD; u++ )
 					{
 						int const x = warp + u * nw;
-						pd[u] = -1;
-						pw[u] = 0.0f;
+#pragma unroll
+						for( int h = 0; h < 2; h++ )
+						{
+							pd[u][h] = -1;
+							pw[u][h] = 0.0f;
+						}
 						if( x < mc )
 						{
 							stage_e const e = sb[c0 + x];
-							int const j = e.lo + lane;
-							if( j < e.hi )
+#pragma unroll
+							for( int h = 0; h < 2; h++ )
 							{
-								pd[u] = __ldg( p.edges + (long long)e.src * p.width + j );
-								pw[u] = q.W[(long long)e.src * p.width + j];
+								int const j = e.lo + lane + 32 * h;
+								if( j < e.hi )
+								{
+									pd[u][h] = __ldg( p.edges + (long long)e.src * p.width + j );
+									pw[u][h] = q.W[(long long)e.src * p.width + j];
+								}
 							}
 						}
 					}
 					// spike x of the chunk into its weight column; (d1st, w1st) = its first slice
 					// element if loaded ahead (ahead1st)
-					auto arrive = [&]( int x, bool ahead1st, int d1st, float w1st ) {
+					auto arrive = [&]( int x, bool ahead1st, int d1st, float w1st, int d2nd, float w2nd ) {
 						stage_e const e = sb[c0 + x];
 						int const rf_off = e.meta & 0xff;
 						bool const replay = rf_off > 0 && Syn::plastic_src( e.src, info );
@@ -429,15 +438,16 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 						unsigned long long const wm = rf_off >= 64 ? ~0ull : ( ( 1ull << rf_off ) - 1 );
 						for( int j = e.lo + lane; j < e.hi; j += 32 )
 						{
-							bool const ahead = ahead1st && j == e.lo + lane;
-							int const d = ahead ? d1st : __ldg( row + j );
+							int const it = ( j - e.lo - lane ) >> 5; // 0: first element of this lane, 1: second
+							bool const ahead = ahead1st && it < 2;
+							int const d = ahead ? ( it == 0 ? d1st : d2nd ) : __ldg( row + j );
 							int const local = d - d0;
 							if( (unsigned)local >= (unsigned)span )
 							{
 								atomicOr( p.err, ERR_BAD_TARGET );
 								continue;
 							}
-							float w = ahead ? w1st : wrow[j];
+							float w = ahead ? ( it == 0 ? w1st : w2nd ) : wrow[j];
 							if( replay && Syn::plastic_dst( d, info ) )
 							{
 								unsigned long long const hb = sh_hist[local] & wm;
@@ -455,9 +465,9 @@ __global__ void __launch_bounds__( 512, 1 ) window_plastic( net_params p, plasti
 					};
 #pragma unroll
 					for( int u = 0; u < PL_AHEAD; u++ )
-						if( warp + u * nw < mc ) arrive( warp + u * nw, true, pd[u], pw[u] );
+						if( warp + u * nw < mc ) arrive( warp + u * nw, true, pd[u][0], pw[u][0], pd[u][1], pw[u][1] );
 					// narrow CTAs (fewer than four warps): the rest without loads ahead
-					for( int x = warp + PL_AHEAD * nw; x < mc; x += nw ) arrive( x, false, 0, 0.0f );
+					for( int x = warp + PL_AHEAD * nw; x < mc; x += nw ) arrive( x, false, 0, 0.0f, 0, 0.0f );
 					__syncthreads();
 					// every target adds its inputs in ascending source order
 #pragma unroll
