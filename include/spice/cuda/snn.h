@@ -114,7 +114,7 @@ public:
 		out->resize( count );
 	}
 
-	// nsteps x step(nullptr), CUDA-graph windows
+	// nsteps x step(nullptr): one cooperative launch, or CUDA-graph windows
 	void run( std::uint64_t nsteps ) { check( spk_net_run( _net, nsteps ) ); }
 
 	std::size_t num_neurons() const override { return info().num_neurons; }

@@ -170,8 +170,10 @@ int spk_net_destroy( spk_net * net );
  * order; *out_count receives their number (SPK_ERR_CAPACITY if > cap). */
 int spk_net_step( spk_net * net, int32_t * out_ids, uint64_t cap, uint64_t * out_count );
 
-/* Advance `nsteps` steps: the same as nsteps calls of step(nullptr), launched as
- * delay-step windows replayed from a CUDA graph. */
+/* Advance `nsteps` steps: the same as nsteps calls of step(nullptr). Non-plastic nets
+ * whose tiles fit the GPU at once run them as one cooperative launch (tiles wait, bounded,
+ * for the spikes they read); other nets as delay-step windows replayed from a CUDA graph.
+ * spk_net_info reports which (persistent) and the launches made (kernel_launches). */
 int spk_net_run( spk_net * net, uint64_t nsteps );
 
 /* Advance `nsteps` steps and return their spike raster to host memory: counts[k] = number

@@ -6,7 +6,7 @@ Mirrors the reference's interface (spice/snn.h, spice/cuda/snn.h, spice/util/lay
     from spice_b200 import Layout, Snn
     net = Snn("brunel", Layout([70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)]), dt=1e-4, delay=15)
     spikes = net.step(out=True)          # snn::step(std::vector<int>*)
-    net.run(100_000)                     # 100k x step(nullptr), CUDA-graph windows
+    net.run(100_000)                     # 100k x step(nullptr): one persistent launch or graph windows
     edges, width = net.adj()             # snn::adj()
     V, Twait = net.neurons()             # snn::neurons() as structure of arrays
 
