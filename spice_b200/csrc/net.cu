@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -83,27 +84,55 @@ int guarded( F && f )
 	}
 }
 
+// Where a buffer's memory comes from: cudaMalloc (pool null), or a stream-ordered pool on
+// `stream`. cudaMalloc and cudaFree synchronise the whole device; the pool synchronises
+// nothing beyond the stream, so a net built or freed beside a running batch does not
+// wait for the batch's launches.
+struct dmem
+{
+	cudaMemPool_t pool = nullptr;
+	cudaStream_t stream = nullptr;
+};
+
 // device allocation owned by the net
 struct dbuf
 {
 	void * p = nullptr;
 	size_t bytes = 0;
+	dmem src{};
 	dbuf() = default;
 	dbuf( dbuf const & ) = delete;
 	dbuf & operator=( dbuf const & ) = delete;
 	~dbuf() { reset(); }
 	void reset()
 	{
-		if( p ) cudaFree( p );
+		if( p )
+		{
+			if( src.pool )
+				cudaFreeAsync( p, src.stream );
+			else
+				cudaFree( p );
+		}
 		p = nullptr;
 		bytes = 0;
+		src = {};
 	}
-	void alloc( size_t b )
+	void alloc( size_t b, dmem m = {} )
 	{
 		reset();
 		if( b == 0 ) return;
-		CK( cudaMalloc( &p, b ) );
+		if( m.pool )
+			CK( cudaMallocFromPoolAsync( &p, b, m.pool, m.stream ) );
+		else
+			CK( cudaMalloc( &p, b ) );
 		bytes = b;
+		src = m;
+	}
+	void swap( dbuf & o )
+	{
+		std::swap( p, o.p );
+		std::swap( bytes, o.bytes );
+		std::swap( src, o.src );
 	}
 	template <typename T>
 	T * as() const
@@ -196,6 +225,20 @@ struct sbuf
 	}
 };
 
+// A kernel's dynamic shared-memory limit on `device` (the current device), set once: the
+// value depends on the kernel and the device only, so nets configured later (beside
+// running launches of the same kernel) make no further driver call for it.
+void set_smem_limit( void const * kernel, int device, int bytes )
+{
+	static std::mutex m;
+	static std::map<std::pair<void const *, int>, int> done;
+	std::lock_guard<std::mutex> lk( m );
+	auto it = done.find( { kernel, device } );
+	if( it != done.end() && it->second == bytes ) return;
+	CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes ) );
+	done[{ kernel, device }] = bytes;
+}
+
 // restores the caller's current device on scope exit
 struct device_guard
 {
@@ -208,6 +251,56 @@ struct device_guard
 	~device_guard()
 	{
 		if( prev >= 0 ) cudaSetDevice( prev );
+	}
+};
+
+// Idle net streams kept for reuse, per device (all of the greatest priority). Creating a
+// stream beside running work took milliseconds in the serving loop, so the stream of a
+// destroyed net (its work synchronised, its buffers' releases issued on it) serves the
+// next net of the device; later work on it is ordered after those releases.
+class stream_recycler
+{
+public:
+	// a stream of the current device, `device`
+	static cudaStream_t take( int device )
+	{
+		{
+			std::lock_guard<std::mutex> lk( mu() );
+			auto & v = idle()[device];
+			if( !v.empty() )
+			{
+				cudaStream_t const s = v.back();
+				v.pop_back();
+				return s;
+			}
+		}
+		int least = 0, greatest = 0;
+		CK( cudaDeviceGetStreamPriorityRange( &least, &greatest ) );
+		cudaStream_t s = nullptr;
+		CK( cudaStreamCreateWithPriority( &s, cudaStreamNonBlocking, greatest ) );
+		return s;
+	}
+	static void give( int device, cudaStream_t s )
+	{
+		std::lock_guard<std::mutex> lk( mu() );
+		auto & v = idle()[device];
+		if( v.size() < KEEP )
+			v.push_back( s );
+		else
+			cudaStreamDestroy( s );
+	}
+
+private:
+	static constexpr size_t KEEP = 256;
+	static std::mutex & mu()
+	{
+		static std::mutex m;
+		return m;
+	}
+	static std::map<int, std::vector<cudaStream_t>> & idle()
+	{
+		static std::map<int, std::vector<cudaStream_t>> m;
+		return m;
 	}
 };
 
@@ -291,10 +384,23 @@ tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 
 struct spk_net
 {
+	// owns `stream` (handed back to the device's stream_recycler); the first member, so
+	// destroyed last: buffers from the pool are released on the stream when the members
+	// after it are destroyed
+	struct stream_owner
+	{
+		int device = 0;
+		cudaStream_t s = nullptr;
+		~stream_owner()
+		{
+			if( s ) stream_recycler::give( device, s );
+		}
+	} owner;
 	int model = 0;
 	int device = 0;
 	int sms = 148;
 	cudaStream_t stream = nullptr;
+	cudaMemPool_t pool = nullptr; // null: cudaMalloc; else the net's buffers come from this pool on `stream`
 	long long n = 0, width = 0;
 	int delay = 1;
 	float dt = 0;
@@ -334,8 +440,9 @@ struct spk_net
 	{
 		if( graph ) cudaGraphExecDestroy( graph );
 		pinned_slots::put( host_count );
-		if( stream ) cudaStreamDestroy( stream );
 	}
+
+	dmem mem() const { return { pool, stream }; }
 
 	spk::net_params params() const
 	{
@@ -427,13 +534,12 @@ struct spk_net
 				CK( cudaFuncGetAttributes( &fa, spk::window_flat<Model> ) );
 				flat_smem = optin - (int)fa.sharedSizeBytes;
 				require( (size_t)flat_smem >= spk::flat_smem_bytes( classes(), neuron_attrs(), flat_tmax ), "shared memory too small for the tiling" );
-				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
 				cudaFuncAttributes fb{};
 				CK( cudaFuncGetAttributes( &fb, spk::window_flat_batch<Model> ) );
 				require( (int)fb.sharedSizeBytes <= (int)fa.sharedSizeBytes + (int)sizeof( spk::net_params ) + 256, "batched kernel shared memory" );
 				flat_smem = std::min( flat_smem, optin - (int)fb.sharedSizeBytes );
-				CK( cudaFuncSetAttribute( spk::window_flat<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
-				CK( cudaFuncSetAttribute( spk::window_flat_batch<Model>, cudaFuncAttributeMaxDynamicSharedMemorySize, flat_smem ) );
+				set_smem_limit( (void const *)spk::window_flat<Model>, device, flat_smem );
+				set_smem_limit( (void const *)spk::window_flat_batch<Model>, device, flat_smem );
 				// one launch for a whole run: every tile's CTA resident at once (cooperative
 				// launch), and the step pipeline never waits on a step not yet simulated
 				int coop = 0, per_sm = 0;
@@ -452,7 +558,7 @@ struct spk_net
 			CK( cudaFuncGetAttributes( &fa, kernel ) );
 			int const limit = optin - (int)fa.sharedSizeBytes;
 			require( smem <= limit, "shared memory too small for the tiling" );
-			CK( cudaFuncSetAttribute( kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit ) );
+			set_smem_limit( (void const *)kernel, device, limit );
 		} );
 	}
 
@@ -556,8 +662,8 @@ struct spk_net
 		if( slots <= ring_slots ) return;
 		require( flat && model != SPK_BRUNEL_PLUS && launched == steps, "ring growth of a window_flat net between runs" );
 		dbuf ids, cnt;
-		ids.alloc( (size_t)slots * n * 4 );
-		cnt.alloc( (size_t)slots * tc.ntiles * 4 );
+		ids.alloc( (size_t)slots * n * 4, mem() );
+		cnt.alloc( (size_t)slots * tc.ntiles * 4, mem() );
 		CK( cudaMemsetAsync( cnt.p, 0, cnt.bytes, stream ) );
 		long long const t = (long long)launched;
 		for( long long st = std::max( 0LL, t - ring_slots ); st < t; st++ )
@@ -568,10 +674,8 @@ struct spk_net
 			                     cudaMemcpyDeviceToDevice, stream ) );
 		}
 		CK( cudaStreamSynchronize( stream ) );
-		std::swap( ring_ids.p, ids.p );
-		std::swap( ring_ids.bytes, ids.bytes );
-		std::swap( ring_cnt.p, cnt.p );
-		std::swap( ring_cnt.bytes, cnt.bytes );
+		ring_ids.swap( ids );
+		ring_cnt.swap( cnt );
 		ring_slots = slots;
 		if( graph ) cudaGraphExecDestroy( graph ); // captured the old ring
 		graph = nullptr;
@@ -801,7 +905,7 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 {
 	net.tile_first_host = first;
 	net.tc.ntiles = (int)first.size() - 1;
-	net.tile_first.alloc( first.size() * 4 );
+	net.tile_first.alloc( first.size() * 4, net.mem() );
 	// on the net's stream (non-blocking: a plain cudaMemcpy from pageable memory may return
 	// before its DMA lands, unordered with the net's kernels)
 	CK( cudaMemcpyAsync( net.tile_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice, net.stream ) );
@@ -923,24 +1027,24 @@ void allocate_buffers( spk_net & net )
 {
 	long long const n = net.n, width = net.width;
 	model_desc const md = describe( net.model );
-	net.edges.alloc( (size_t)( n * width ) * 4 );
-	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4 );
-	net.ring_ids.alloc( (size_t)net.ring_slots * n * 4 );
-	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4 );
-	net.clock.alloc( sizeof( spk::clock_state ) );
-	net.dt_ring.alloc( spk::DT_RING * 4 );
-	net.err.alloc( 4 );
-	for( int i = 0; i < md.neuron_attrs; i++ ) net.attr[i].alloc( (size_t)n * 4 );
-	net.gather_ids.alloc( (size_t)n * 4 );
-	net.gather_cnt.alloc( 4 );
-	net.cursor.alloc( 8 );
-	net.gather_done.alloc( 4 );
+	net.edges.alloc( (size_t)( n * width ) * 4, net.mem() );
+	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4, net.mem() );
+	net.ring_ids.alloc( (size_t)net.ring_slots * n * 4, net.mem() );
+	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4, net.mem() );
+	net.clock.alloc( sizeof( spk::clock_state ), net.mem() );
+	net.dt_ring.alloc( spk::DT_RING * 4, net.mem() );
+	net.err.alloc( 4, net.mem() );
+	for( int i = 0; i < md.neuron_attrs; i++ ) net.attr[i].alloc( (size_t)n * 4, net.mem() );
+	net.gather_ids.alloc( (size_t)n * 4, net.mem() );
+	net.gather_cnt.alloc( 4, net.mem() );
+	net.cursor.alloc( 8, net.mem() );
+	net.gather_done.alloc( 4, net.mem() );
 	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
 	CK( cudaMemsetAsync( net.clock.p, 0, net.clock.bytes, net.stream ) );
 	CK( cudaMemsetAsync( net.err.p, 0, 4, net.stream ) );
 	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
 	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
-	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream );
+	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream, net.pool );
 	if( !net.host_count ) net.host_count = pinned_slots::get();
 	net.configure();
 }
@@ -963,8 +1067,8 @@ void build_slices( spk_net & net )
 {
 	int const nt = net.tc.ntiles;
 	long long const n = net.n;
-	net.slice_rec.alloc( (size_t)n * nt * sizeof( uint2 ) );
-	net.tile_inputs.alloc( (size_t)nt * 4 );
+	net.slice_rec.alloc( (size_t)n * nt * sizeof( uint2 ), net.mem() );
+	net.tile_inputs.alloc( (size_t)nt * 4, net.mem() );
 	CK( cudaMemsetAsync( net.tile_inputs.p, 0, net.tile_inputs.bytes, net.stream ) );
 	sbuf rows( (size_t)n * 4, net.stream, net.device ), bases( (size_t)n * 8, net.stream, net.device );
 	std::vector<unsigned> rv( n );
@@ -986,9 +1090,9 @@ void build_slices( spk_net & net )
 	require( all < ( 1ULL << 32 ), "graph too large for 32-bit slice records" );
 	char const * sync = getenv( "SPK_FLAT_SYNC" );
 	net.flat_sync = sync && !strcmp( sync, "1" );
-	net.done_step.alloc( (size_t)nt * sizeof( long long ) );
+	net.done_step.alloc( (size_t)nt * sizeof( long long ), net.mem() );
 	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
-	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ) );
+	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ), net.mem() );
 	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)n * 8, cudaMemcpyHostToDevice, net.stream ) );
 	switch( net.model )
 	{
@@ -1026,8 +1130,8 @@ void retile( spk_net & net, int target )
 	for( size_t i = 0; i < net.seg_start.size(); i++ ) segs.push_back( { (long long)net.seg_start[i], net.seg_cost[i] } );
 	CK( cudaStreamSynchronize( net.stream ) );
 	require( flat_tiling( net, segs, target ), "tiling failed" );
-	net.pivots.alloc( (size_t)net.n * ( net.tc.ntiles + 1 ) * 4 );
-	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4 );
+	net.pivots.alloc( (size_t)net.n * ( net.tc.ntiles + 1 ) * 4, net.mem() );
+	net.ring_cnt.alloc( (size_t)net.ring_slots * net.tc.ntiles * 4, net.mem() );
 	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
 	enqueue_pivots( net );
 	if( net.graph ) cudaGraphExecDestroy( net.graph );
@@ -1036,14 +1140,14 @@ void retile( spk_net & net, int target )
 	CK( cudaStreamSynchronize( net.stream ) );
 }
 
-void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned long long seed, int * d_edges, dbuf & conns_dev )
+void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned long long seed, int * d_edges, dbuf & conns_dev, dmem m = {} )
 {
 	std::vector<spk::conn_dev> cs;
 	for( auto const & c : l.connections() )
 		cs.push_back( { std::get<0>( c ), std::get<1>( c ), std::get<2>( c ), std::get<3>( c ), bernoulli_threshold( std::get<4>( c ) ) } );
 	long long const n = (long long)l.size(), w = (long long)l.max_degree();
 	if( n == 0 || w == 0 ) return;
-	conns_dev.alloc( std::max<size_t>( cs.size(), 1 ) * sizeof( spk::conn_dev ) );
+	conns_dev.alloc( std::max<size_t>( cs.size(), 1 ) * sizeof( spk::conn_dev ), m );
 	if( !cs.empty() ) CK( cudaMemcpyAsync( conns_dev.p, cs.data(), cs.size() * sizeof( spk::conn_dev ), cudaMemcpyHostToDevice, s ) );
 	int const blocks = (int)( ( n * 32 + 255 ) / 256 );
 	spk::generate_ell<<<blocks, 256, 0, s>>>( (int)n, (int)w, (int)cs.size(), conns_dev.as<spk::conn_dev>(), seed, d_edges );
@@ -1180,9 +1284,9 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	device_guard g( device ); // the stream belongs to the net's device
 	// a net's own work (building it, its windows, exports) at the highest stream priority:
 	// beside the long shared launches of a batch its CTAs start as soon as an SM frees up
-	int least = 0, greatest = 0;
-	CK( cudaDeviceGetStreamPriorityRange( &least, &greatest ) );
-	CK( cudaStreamCreateWithPriority( &net->stream, cudaStreamNonBlocking, greatest ) );
+	net->stream = stream_recycler::take( device );
+	net->owner.device = device;
+	net->owner.s = net->stream;
 	return net.release();
 }
 } // namespace
@@ -1379,6 +1483,35 @@ struct spk_batch
 
 namespace
 {
+int create_net(
+    spk_net ** out,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    int device,
+    int tile_target,
+    bool pooled )
+{
+	return guarded( [&] {
+		require( out != nullptr, "out is null" );
+		require( tile_target >= 0, "tile target must be >= 0" );
+		*out = nullptr;
+		auto const l = to_layout( desc );
+		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
+		device_guard g( device );
+		if( pooled ) net->pool = scratch_pool( device );
+		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ), tile_target );
+		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev, net->mem() );
+		enqueue_pivots( *net );
+		init_state( *net );
+		CK( cudaStreamSynchronize( net->stream ) );
+		*out = net.release();
+	} );
+}
+
 void detach( spk_batch * b, spk_net * net )
 {
 	b->nets.erase( std::remove( b->nets.begin(), b->nets.end(), net ), b->nets.end() );
@@ -1387,6 +1520,53 @@ void detach( spk_batch * b, spk_net * net )
 } // namespace
 
 void spk_set_last_error( std::string const & msg ) { g_err = msg; }
+
+// A net whose buffers come from the device's stream-ordered pool (on the net's stream):
+// neither building nor destroying it synchronises the device, so the server's builder
+// does not wait for the launches of the nets it steps meanwhile.
+int spk_net_create_pooled(
+    spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target )
+{
+	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, tile_target, true );
+}
+
+// Maps up to `bytes` (at most the device's free memory less 1 GiB) into the device's
+// stream-ordered pool ahead of use: the pool keeps released memory, so nets built from it
+// later reuse mapped memory instead of growing the pool beside running work (growing it
+// took tens of milliseconds per net in the serving loop). Best effort: a failed
+// reservation leaves the pool to grow on demand.
+void spk_reserve_pool( int device, uint64_t bytes )
+{
+	int ndev = 0;
+	if( cudaGetDeviceCount( &ndev ) != cudaSuccess || device < 0 || device >= ndev ) return;
+	try
+	{
+		device_guard g( device );
+		size_t free_b = 0, total_b = 0;
+		if( cudaMemGetInfo( &free_b, &total_b ) != cudaSuccess ) return;
+		size_t const margin = (size_t)1 << 30;
+		size_t const size = std::min<size_t>( bytes, free_b > margin ? free_b - margin : 0 );
+		if( size == 0 ) return;
+		cudaStream_t s = stream_recycler::take( device );
+		void * p = nullptr;
+		if( cudaMallocFromPoolAsync( &p, size, scratch_pool( device ), s ) == cudaSuccess ) cudaFreeAsync( p, s );
+		cudaGetLastError();
+		cudaStreamSynchronize( s );
+		stream_recycler::give( device, s );
+	}
+	catch( ... )
+	{
+		cudaGetLastError();
+	}
+}
+
+// hands the pool's unused memory back to the device (after a server's nets are gone)
+void spk_trim_pool( int device )
+{
+	int ndev = 0;
+	if( cudaGetDeviceCount( &ndev ) != cudaSuccess || device < 0 || device >= ndev ) return;
+	cudaMemPoolTrimTo( scratch_pool( device ), 0 );
+}
 
 extern "C" {
 char const * spk_last_error( void ) { return g_err.c_str(); }
@@ -1438,20 +1618,7 @@ int spk_net_create( spk_net ** out, int model, spk_layout_desc const * desc, flo
 int spk_net_create_ex(
     spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target )
 {
-	return guarded( [&] {
-		require( out != nullptr, "out is null" );
-		require( tile_target >= 0, "tile target must be >= 0" );
-		*out = nullptr;
-		auto const l = to_layout( desc );
-		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
-		device_guard g( device );
-		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ), tile_target );
-		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev );
-		enqueue_pivots( *net );
-		init_state( *net );
-		CK( cudaStreamSynchronize( net->stream ) );
-		*out = net.release();
-	} );
+	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, tile_target, false );
 }
 
 int spk_net_estimate_bytes( int model, spk_layout_desc const * desc, int delay, int device, int tile_target, uint64_t * out_bytes )
@@ -1590,8 +1757,8 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 			if( out_total ) *out_total = 0;
 			return;
 		}
-		if( net->rec_ids.bytes < std::max<uint64_t>( ids_cap, 1 ) * 4 ) net->rec_ids.alloc( std::max<uint64_t>( ids_cap, 1 ) * 4 );
-		if( net->rec_cnt.bytes < nsteps * 4 ) net->rec_cnt.alloc( nsteps * 4 );
+		if( net->rec_ids.bytes < std::max<uint64_t>( ids_cap, 1 ) * 4 ) net->rec_ids.alloc( std::max<uint64_t>( ids_cap, 1 ) * 4, net->mem() );
+		if( net->rec_cnt.bytes < nsteps * 4 ) net->rec_cnt.alloc( nsteps * 4, net->mem() );
 		CK( cudaMemsetAsync( net->cursor.p, 0, 8, net->stream ) );
 		// persistent nets record in chunks: one launch per chunk into a ring enlarged to
 		// hold the chunk (bounded to RECORD_RING_BYTES), one gather per chunk

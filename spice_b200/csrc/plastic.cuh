@@ -773,31 +773,46 @@ inline int plastic_window_smem( int tile, int ntiles, int threads )
 // device buffers of the plastic state
 struct plastic_state
 {
+	// from cudaMalloc, or (pool set) from a stream-ordered pool on stream s
 	struct buf
 	{
 		void * p = nullptr;
 		size_t bytes = 0;
-		~buf()
+		cudaMemPool_t pool = nullptr;
+		cudaStream_t s = nullptr;
+		~buf() { release(); }
+		void release()
 		{
-			if( p ) cudaFree( p );
-		}
-		void alloc( size_t b )
-		{
-			if( p ) cudaFree( p );
+			if( p )
+			{
+				if( pool )
+					cudaFreeAsync( p, s );
+				else
+					cudaFree( p );
+			}
 			p = nullptr;
 			bytes = 0;
+		}
+		void alloc( size_t b, cudaMemPool_t from, cudaStream_t on )
+		{
+			release();
 			if( !b ) return;
-			cudaError_t const e = cudaMalloc( &p, b );
+			cudaError_t const e = from ? cudaMallocFromPoolAsync( &p, b, from, on ) : cudaMalloc( &p, b );
 			if( e != cudaSuccess )
 			{
+				p = nullptr;
 				cudaGetLastError();
 				throw std::bad_alloc();
 			}
 			bytes = b;
+			pool = from;
+			s = on;
 		}
 	};
 	buf W, za, zpre, zpost, hist, rf_a, zrf_a, rf_c, zrf_c, ring_meta, flush_ring, flush_cnt, ring_pot, tmp;
 	bool active = false;
+	cudaMemPool_t pool = nullptr; // where the buffers come from (null: cudaMalloc)
+	cudaStream_t stream = nullptr;
 
 	size_t bytes() const
 	{
@@ -805,22 +820,24 @@ struct plastic_state
 		       ring_meta.bytes + flush_ring.bytes + flush_cnt.bytes + ring_pot.bytes + tmp.bytes;
 	}
 
-	void allocate( long long n, long long width, int ntiles, int delay, cudaStream_t stream )
+	void allocate( long long n, long long width, int ntiles, int delay, cudaStream_t stream, cudaMemPool_t from )
 	{
 		active = true;
-		W.alloc( (size_t)( n * width ) * 4 );
-		za.alloc( n * 4 );
-		zpre.alloc( n * 4 );
-		zpost.alloc( n * 4 );
-		hist.alloc( n * 8 );
-		rf_a.alloc( n * 4 );
-		zrf_a.alloc( n * 4 );
-		rf_c.alloc( n * 4 );
-		zrf_c.alloc( n * 4 );
-		ring_meta.alloc( (size_t)2 * delay * n * 16 );
-		flush_ring.alloc( (size_t)2 * delay * n * 16 );
-		flush_cnt.alloc( (size_t)2 * delay * ntiles * 4 );
-		ring_pot.alloc( (size_t)2 * delay * ntiles * 4 );
+		pool = from;
+		this->stream = stream;
+		W.alloc( (size_t)( n * width ) * 4, pool, stream );
+		za.alloc( n * 4, pool, stream );
+		zpre.alloc( n * 4, pool, stream );
+		zpost.alloc( n * 4, pool, stream );
+		hist.alloc( n * 8, pool, stream );
+		rf_a.alloc( n * 4, pool, stream );
+		zrf_a.alloc( n * 4, pool, stream );
+		rf_c.alloc( n * 4, pool, stream );
+		zrf_c.alloc( n * 4, pool, stream );
+		ring_meta.alloc( (size_t)2 * delay * n * 16, pool, stream );
+		flush_ring.alloc( (size_t)2 * delay * n * 16, pool, stream );
+		flush_cnt.alloc( (size_t)2 * delay * ntiles * 4, pool, stream );
+		ring_pot.alloc( (size_t)2 * delay * ntiles * 4, pool, stream );
 		// on the net's stream, ahead of the kernels that read them
 		cudaMemsetAsync( flush_cnt.p, 0, flush_cnt.bytes, stream );
 		cudaMemsetAsync( ring_pot.p, 0, ring_pot.bytes, stream );
@@ -879,7 +896,7 @@ struct plastic_state
 	{
 		long long const ne = (long long)p.n * p.width;
 		if( ne == 0 ) return cudaSuccess;
-		if( tmp.bytes < (size_t)ne * 4 ) tmp.alloc( (size_t)ne * 4 );
+		if( tmp.bytes < (size_t)ne * 4 ) tmp.alloc( (size_t)ne * 4, pool, stream );
 		float * t = static_cast<float *>( tmp.p );
 		cudaMemcpyAsync( t, W.p, ne * 4, cudaMemcpyDeviceToDevice, s );
 		settle_weights<Model><<<p.n, 256, 0, s>>>( p, params(), t );

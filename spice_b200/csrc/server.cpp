@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -31,14 +32,24 @@
 #include <thread>
 #include <vector>
 
-// the library's per-thread error message (spk_last_error), defined with the C ABI
+// defined in net.cu beside the C ABI: the per-thread error message (spk_last_error), nets
+// built from the device's stream-ordered pool, and handing that pool's unused memory back
 void spk_set_last_error( std::string const & msg );
+int spk_net_create_pooled(
+    spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target );
+void spk_trim_pool( int device );
+void spk_reserve_pool( int device, uint64_t bytes );
 
 namespace
 {
-// builder threads (one: concurrent builds measured slower, their device-wide
-// synchronisations -- allocations, frees -- queue behind each other and the ticker's work)
-constexpr int BUILDERS = 1;
+// builder threads: SPK_SERVER_BUILDERS (1-8), default 2 (with jobs queued, a second
+// builder overlaps one build's host work with another's kernels)
+int builders_count()
+{
+	char const * e = getenv( "SPK_SERVER_BUILDERS" );
+	int const n = e ? atoi( e ) : 2;
+	return n < 1 ? 1 : ( n > 8 ? 8 : n );
+}
 
 int fail( int code, std::string const & msg )
 {
@@ -100,7 +111,7 @@ struct server
 	uint64_t in_use = 0, peak = 0, ticks = 0;
 	double build_s = 0, tick_s = 0;
 	int inject = 0;
-	std::vector<std::thread> builders; // BUILDERS threads admit and build concurrently
+	std::vector<std::thread> builders; // builders_count() threads admit and build concurrently
 	std::thread ticker;
 
 	double now() const { return std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count(); }
@@ -127,7 +138,8 @@ struct server
 	int build( job & j, int target, std::string & msg )
 	{
 		auto const d = j.desc();
-		int const rc = spk_net_create_ex( &j.net, j.model, &d, j.dt, j.delay, j.seed, j.graph_seed, device, target );
+		// from the stream-ordered pool: no device-wide synchronisation while the ticker runs
+		int const rc = spk_net_create_pooled( &j.net, j.model, &d, j.dt, j.delay, j.seed, j.graph_seed, device, target );
 		if( rc != SPK_OK )
 		{
 			msg = spk_last_error();
@@ -404,7 +416,9 @@ int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uin
 		return fail( SPK_ERR_INVALID, "invalid device" );
 	int const rc = spk_batch_create( &s->batch, device );
 	if( rc != SPK_OK ) return rc;
-	for( int b = 0; b < BUILDERS; b++ ) s->builders.emplace_back( [p = s.get()] { p->build_loop(); } );
+	// the budget mapped into the pool the nets are built from, before any job runs
+	spk_reserve_pool( device, budget_bytes );
+	for( int b = 0, nb = builders_count(); b < nb; b++ ) s->builders.emplace_back( [p = s.get()] { p->build_loop(); } );
 	s->ticker = std::thread( [p = s.get()] { p->tick_loop(); } );
 	*out = s.release();
 	return SPK_OK;
@@ -605,7 +619,9 @@ int spk_server_destroy( spk_server * s )
 		j->net = nullptr;
 	}
 	spk_batch_destroy( s->batch );
+	int const device = s->device;
 	delete s;
+	spk_trim_pool( device );
 	return SPK_OK;
 }
 }
