@@ -183,7 +183,9 @@ int spk_net_run( spk_net * net, uint64_t nsteps );
 int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32_t * ids, uint64_t ids_cap, uint64_t * out_total );
 
 /* The CUDA stream (cudaStream_t) every kernel of this net runs on, for callers that order
- * their own work or record events against it. Queued steps are launched first. */
+ * their own work or record events against it. Queued steps are launched first. The stream
+ * belongs to the library: do not destroy it; after spk_net_destroy it serves later nets
+ * of the device. */
 int spk_net_stream( spk_net * net, void ** out_stream );
 
 /* Wait for all queued work; reports device-side errors. */
