@@ -514,6 +514,11 @@ def run_serving(args, rank, world):
     srv.close()
     clk = clocks.stop()
     states = [i.state for i in infos]
+    failures = {}  # "state error: message" of every job that did not complete, with counts
+    for i in infos:
+        if i.state != 2:
+            key = f"{i.state} {i.error}: {i.message.decode(errors='replace')}"
+            failures[key] = failures.get(key, 0) + 1
     lat = [i.t_end - i.t_submit for i in infos if i.state == 2]
     first = min(i.t_submit for i in infos)
     span = max(i.t_end for i in infos) - first
@@ -526,6 +531,7 @@ def run_serving(args, rank, world):
                            "syn_range": [1e6, 2e8], "bio_range_s": [0.1, 2.0], "arrival_s": args.duration,
                            "budget_gb": args.budget_gb, "quantum_steps": args.quantum},
                 "server": {"p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "span_s": span, "done": states.count(2),
+                           "not_done": failures,
                            "sims_per_s": states.count(2) / span, "synapse_steps_per_s": syn_steps / span,
                            "peak_gb": st["peak_bytes"] / 1e9, "ticks": st["ticks"],
                            "build_s": st["build_seconds"], "tick_s": st["tick_seconds"]},
