@@ -254,10 +254,12 @@ struct device_guard
 	}
 };
 
-// Idle net streams kept for reuse, per device (all of the greatest priority). Creating a
-// stream beside running work took milliseconds in the serving loop, so the stream of a
-// destroyed net (its work synchronised, its buffers' releases issued on it) serves the
-// next net of the device; later work on it is ordered after those releases.
+// Idle streams of the serving loop's nets kept for reuse, per device (all of the greatest
+// priority). Creating a stream beside running work took milliseconds in the serving loop,
+// so the stream of a destroyed net (its work synchronised, its buffers' releases issued
+// on it) serves the next such net of the device; later work on it is ordered after those
+// releases. Nets outside the server do not use it: measured alone, their destruction
+// took twice as long with recycled streams.
 class stream_recycler
 {
 public:
@@ -384,16 +386,21 @@ tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 
 struct spk_net
 {
-	// owns `stream` (handed back to the device's stream_recycler); the first member, so
-	// destroyed last: buffers from the pool are released on the stream when the members
-	// after it are destroyed
+	// owns `stream` (destroyed, or handed back to the device's stream_recycler if it came
+	// from there); the first member, so destroyed last: buffers from the pool are released
+	// on the stream when the members after it are destroyed
 	struct stream_owner
 	{
 		int device = 0;
+		bool recycle = false;
 		cudaStream_t s = nullptr;
 		~stream_owner()
 		{
-			if( s ) stream_recycler::give( device, s );
+			if( !s ) return;
+			if( recycle )
+				stream_recycler::give( device, s );
+			else
+				cudaStreamDestroy( s );
 		}
 	} owner;
 	int model = 0;
@@ -1266,7 +1273,10 @@ std::vector<std::pair<uint32_t, spk::plastic_state::buf *>> ckpt_plastic( spk_ne
 	         { 50, &q.flush_ring }, { 51, &q.flush_cnt }, { 52, &q.ring_pot } };
 }
 
-spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int device )
+// pooled: the net's buffers come from the device's stream-ordered pool and its stream
+// from the stream_recycler (the serving loop's nets); otherwise cudaMalloc and a stream
+// of its own, destroyed with the net
+spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int device, bool pooled = false )
 {
 	describe( model );
 	require( dt > 0.0f, "dt must be > 0" );
@@ -1284,9 +1294,18 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	device_guard g( device ); // the stream belongs to the net's device
 	// a net's own work (building it, its windows, exports) at the highest stream priority:
 	// beside the long shared launches of a batch its CTAs start as soon as an SM frees up
-	net->stream = stream_recycler::take( device );
 	net->owner.device = device;
-	net->owner.s = net->stream;
+	net->owner.recycle = pooled;
+	if( pooled )
+		net->owner.s = stream_recycler::take( device );
+	else
+	{
+		int least = 0, greatest = 0;
+		CK( cudaDeviceGetStreamPriorityRange( &least, &greatest ) );
+		CK( cudaStreamCreateWithPriority( &net->owner.s, cudaStreamNonBlocking, greatest ) );
+	}
+	net->stream = net->owner.s;
+	if( pooled ) net->pool = scratch_pool( device );
 	return net.release();
 }
 } // namespace
@@ -1500,9 +1519,8 @@ int create_net(
 		require( tile_target >= 0, "tile target must be >= 0" );
 		*out = nullptr;
 		auto const l = to_layout( desc );
-		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
+		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device, pooled ) );
 		device_guard g( device );
-		if( pooled ) net->pool = scratch_pool( device );
 		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ), tile_target );
 		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev, net->mem() );
 		enqueue_pivots( *net );
