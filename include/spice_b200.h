@@ -184,8 +184,8 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 
 /* The CUDA stream (cudaStream_t) every kernel of this net runs on, for callers that order
  * their own work or record events against it. Queued steps are launched first. The stream
- * belongs to the library: do not destroy it; after spk_net_destroy it serves later nets
- * of the device. */
+ * belongs to the library: do not destroy it (spk_net_destroy does; a server's nets hand
+ * theirs on to the server's later nets). */
 int spk_net_stream( spk_net * net, void ** out_stream );
 
 /* Wait for all queued work; reports device-side errors. */
