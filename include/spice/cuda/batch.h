@@ -46,6 +46,8 @@ private:
 class server
 {
 public:
+	// maps the budget into the device's stream-ordered pool the jobs' nets are built from
+	// (spk_server_create); the destructor hands it back
 	server( std::uint64_t budget_bytes, std::uint64_t quantum_steps, int device = 0 )
 	{
 		check( spk_server_create( &_s, device, budget_bytes, quantum_steps ) );

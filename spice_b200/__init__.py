@@ -451,6 +451,8 @@ def estimate_bytes(model, layout, delay=1, device=0, tile_target=0):
 class Server:
     """Simulation jobs admitted against a device-memory budget and stepped by continuous
     batching on one GPU (native builder threads and a ticker thread; see spk_server_* in spice_b200.h).
+    Creation maps the budget (at most the free memory less 1 GiB) into the device's
+    stream-ordered pool, which the jobs' nets are built from; close() hands it back.
 
     srv = Server(budget_bytes=150e9, quantum=1500)
     job = srv.submit("brunel", layout, nsteps=10_000, delay=15, seed=1)
