@@ -1,6 +1,6 @@
 """The multi-rank plumbing of bench.py (one process per GPU; replicas only: the path does not
 shard) on CPU: two gloo ranks agree on the max over ranks, meet at barriers, and the
-reference arm runs on rank 0 alone."""
+reference arm runs on rank 0 alone; and the serving workload's seeded job stream."""
 import os
 import socket
 
@@ -47,3 +47,19 @@ def test_two_gloo_ranks_max_and_barrier():
         assert p.exitcode == 0
     res = sorted(q.get(timeout=10) for _ in range(2))
     assert [r[1] for r in res] == [2.5, 2.5] and all(r[2] for r in res)
+
+
+def test_serving_saturation_runs_the_same_jobs():
+    """The serving workload at saturation (--rate 1000 --duration 0.16) submits the very
+    jobs of the 20 jobs/s run (--rate 20 --duration 8), only sooner: the arrival gaps scale
+    with 1/rate while every other draw comes from the same seeded stream."""
+    import sys
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    slow, fast = bench.serving_jobs(20.0, 8.0), bench.serving_jobs(1000.0, 0.16)
+    assert len(slow) == len(fast) == 144
+    for a, b in zip(slow, fast):
+        assert abs(a["t"] / 50.0 - b["t"]) < 1e-9
+        assert {k: v for k, v in a.items() if k != "t"} == {k: v for k, v in b.items() if k != "t"}
