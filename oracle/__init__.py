@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "libspice_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libspice_ref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libspice_ref_fast.so")
-REFERENCE_SRC = "/root/reference"
+# the reference checkout the `ref` build compiles from (no default: set by the build recipe)
+REFERENCE_SRC = os.environ.get("SPICE_REFERENCE_SRC", "")
 
 MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3}
 NEURON_ATTRS = {0: [np.float32] * 3 + [np.int32], 1: [np.float32, np.int32], 2: [np.float32, np.int32], 3: [np.int32]}
@@ -27,11 +28,13 @@ NEURON_ATTRS = {0: [np.float32] * 3 + [np.int32], 1: [np.float32, np.int32], 2: 
 U64P, IP, FP = C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_float)
 
 
-def build(reference=True):
-    """Compile the restatement and, where the reference sources exist, the reference."""
+def build(reference=True, reference_src=None):
+    """Compile the restatement and, where the reference sources exist (reference_src, else
+    the SPICE_REFERENCE_SRC environment variable), the reference."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if reference and os.path.isdir(os.path.join(REFERENCE_SRC, "spice")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}"], check=True)
+    src = reference_src or REFERENCE_SRC
+    if reference and src and os.path.isdir(os.path.join(src, "spice")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
 
 
 def have_reference(fast=False):
@@ -73,6 +76,8 @@ def oracle_lib():
         lib.oracle_synapses_f32.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         lib.oracle_dt_sequence.argtypes = [C.c_float, C.c_int, FP]
         lib.oracle_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        lib.oracle_set_state.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        lib.oracle_set_progress.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_uint32), IP]
         _olib = lib
     return _olib
 
@@ -167,6 +172,23 @@ class OracleNet:
             oracle_lib().oracle_neurons(self._h, (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs]))
         return arrs
 
+    def set_state(self, neurons, synapses=None):
+        """Replace the neuron state (the model's attribute arrays, float32 / int32) and, for
+        Brunel+, the synapse state (W, Zpre, Zpost over all n x width slots, float32)."""
+        na = [np.ascontiguousarray(a, dtype=t) for a, t in zip(neurons, NEURON_ATTRS[self.model])]
+        sa = [np.ascontiguousarray(a, dtype=np.float32) for a in synapses] if synapses else []
+        oracle_lib().oracle_set_state(self._h, (C.c_void_p * len(na))(*[a.ctypes.data for a in na]),
+                                      (C.c_void_p * 3)(*[a.ctypes.data for a in sa]) if sa else None)
+
+    def set_progress(self, step0, counts=(), ids=()):
+        """Continue a run at step `step0` with the spikes of the last len(counts) steps
+        (counts per step, ids concatenated, oldest first) in flight."""
+        c = np.ascontiguousarray(counts, dtype=np.uint32)
+        i = np.ascontiguousarray(ids, dtype=np.int32)
+        if oracle_lib().oracle_set_progress(self._h, int(step0), len(c), c.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                            i.ctypes.data_as(IP)):
+            raise ValueError(oracle_lib().oracle_last_error().decode())
+
     def synapses(self):
         if self.model != 2:
             return []
@@ -200,6 +222,10 @@ def ref_lib(fast=False):
         lib.ref_generate.restype = C.c_uint64
         lib.ref_generate.argtypes = [C.c_int, U64P, C.c_int, IP, IP, FP, IP]
         lib.ref_layout.argtypes = [C.c_int, U64P, C.c_int, IP, IP, FP, IP, FP, C.c_int, U64P, U64P]
+        lib.ref_create_from_state.restype = C.c_void_p
+        lib.ref_create_from_state.argtypes = [C.c_int, C.c_uint64, C.c_uint64, IP, C.POINTER(C.c_void_p),
+                                              C.POINTER(C.c_void_p), C.c_float, C.c_int, C.c_uint64, C.c_uint64,
+                                              C.c_int, C.POINTER(C.c_uint32), IP]
         _rlibs[path] = lib
     return _rlibs[path]
 
@@ -207,16 +233,41 @@ def ref_lib(fast=False):
 class ReferenceNet:
     """The reference's cpu::snn (with the counter-RNG Poisson stream)."""
 
-    def __init__(self, model, pops, conns, dt=1e-4, delay=1, seed=1, fast=False):
+    def __init__(self, model, pops, conns, dt=1e-4, delay=1, seed=1, fast=False, _state=None):
         lib = ref_lib(fast)
         self.lib = lib
         self.model = MODELS[model] if isinstance(model, str) else int(model)
-        self._h = lib.ref_create(self.model, *_layout_args(pops, conns), dt, delay, seed)
+        if _state is None:
+            self._h = lib.ref_create(self.model, *_layout_args(pops, conns), dt, delay, seed)
+        else:
+            edges, width, neurons, synapses, step0, counts, ids = _state
+            e = np.ascontiguousarray(edges, dtype=np.int32)
+            n = e.size // width if width else len(neurons[0])
+            na = [np.ascontiguousarray(a, dtype=t) for a, t in zip(neurons, NEURON_ATTRS[self.model])]
+            sa = [np.ascontiguousarray(a, dtype=np.float32) for a in synapses] if synapses else []
+            c = np.ascontiguousarray(counts, dtype=np.uint32)
+            i = np.ascontiguousarray(ids, dtype=np.int32)
+            self._h = lib.ref_create_from_state(self.model, n, width, e.ctypes.data_as(IP),
+                                                (C.c_void_p * len(na))(*[a.ctypes.data for a in na]),
+                                                (C.c_void_p * 3)(*[a.ctypes.data for a in sa]) if sa else None,
+                                                dt, delay, seed, int(step0), len(c), c.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                i.ctypes.data_as(IP))
         if not self._h:
             raise ValueError(lib.ref_last_error().decode())
         self.n = lib.ref_num_neurons(self._h)
         self.width = lib.ref_width(self._h)
         self._buf = np.empty(max(1, self.n), dtype=np.int32)
+
+    @classmethod
+    def from_state(cls, model, edges, width, neurons, synapses=None, dt=1e-4, delay=1, seed=1, fast=False, step0=0,
+                   counts=(), ids=()):
+        """The reference's cpu::snn over a given graph (n x width ELL) and state (neuron
+        attribute arrays; for Brunel+ also W, Zpre, Zpost over all slots): a simulation that
+        continues where another one stands at step `step0` (clock and Poisson stream keyed by
+        `seed`), with the spikes of the last len(counts) steps in flight (counts per step, ids
+        concatenated, oldest first)."""
+        return cls(model, None, None, dt=dt, delay=delay, seed=seed, fast=fast,
+                   _state=(edges, int(width), neurons, synapses, step0, counts, ids))
 
     def __del__(self):
         if getattr(self, "_h", None):

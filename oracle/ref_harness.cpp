@@ -17,7 +17,9 @@
 #include <exception>
 #include <memory>
 #include <string>
+#include <stdexcept>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace
@@ -56,6 +58,71 @@ void scatter_tuple( std::vector<Tuple> const & v, void ** attrs, std::index_sequ
 	  ... );
 }
 
+// cpu::snn keeps its graph and state private and has no constructor from an adjacency
+// (spice/cpu/snn.h:16-46). The explicit-instantiation rule (template arguments of an
+// explicit instantiation are not access-checked) gives the harness pointers to those three
+// members, so a reference net can start from a given graph and state: the GPU net's state
+// at the same step, for parity checks at sizes where running the reference from step 0 to
+// a steady state takes too long.
+template <typename Tag, auto Member>
+struct member_access
+{
+	friend auto member_pointer( Tag ) { return Member; }
+};
+template <typename Model>
+struct graph_tag
+{
+	friend auto member_pointer( graph_tag );
+};
+template <typename Model>
+struct neurons_tag
+{
+	friend auto member_pointer( neurons_tag );
+};
+template <typename Model>
+struct synapses_tag
+{
+	friend auto member_pointer( synapses_tag );
+};
+template <typename Model>
+struct spikes_tag
+{
+	friend auto member_pointer( spikes_tag );
+};
+template <typename Model>
+struct istep_tag
+{
+	friend auto member_pointer( istep_tag );
+};
+template <typename Model>
+struct simtime_tag
+{
+	friend auto member_pointer( simtime_tag );
+};
+#define SPICE_HARNESS_ACCESS( M )                                                                             \
+	template struct member_access<graph_tag<M>, &spice::cpu::snn<M>::_graph>;                                \
+	template struct member_access<neurons_tag<M>, &spice::cpu::snn<M>::_neurons>;                            \
+	template struct member_access<synapses_tag<M>, &spice::cpu::snn<M>::_synapses>;                          \
+	template struct member_access<spikes_tag<M>, &spice::cpu::snn<M>::_spikes>;                              \
+	template struct member_access<istep_tag<M>, &spice::snn<M>::_i>;                                         \
+	template struct member_access<simtime_tag<M>, &spice::snn<M>::_simtime>;
+SPICE_HARNESS_ACCESS( spice::vogels_abbott )
+SPICE_HARNESS_ACCESS( spice::brunel )
+SPICE_HARNESS_ACCESS( spice::brunel_with_plasticity )
+SPICE_HARNESS_ACCESS( spice::synth )
+#undef SPICE_HARNESS_ACCESS
+
+template <typename Tuple, size_t... I>
+void gather_tuple( std::vector<Tuple> & v, void * const * attrs, std::index_sequence<I...> )
+{
+	( [&] {
+		using T = std::tuple_element_t<I, Tuple>;
+		T const * src = static_cast<T const *>( attrs[I] );
+		for( size_t k = 0; k < v.size(); k++ ) std::get<I>( v[k] ) = src[k];
+	}(),
+	  ... );
+}
+
 template <typename Model>
 struct net : net_base
 {
@@ -65,6 +132,57 @@ struct net : net_base
 	net( spice::util::layout const & l, float dt, int delay )
 	    : impl( l, dt, delay )
 	{
+	}
+
+	// a net of n neurons without synapses, then the given graph (n x width ELL) and state
+	// (one array per attribute, in the model's attribute order) put in its place; with
+	// step0 > 0 the net stands at step step0: its simulated clock advanced by step0 steps
+	// and the spikes of the steps [step0 - nq, step0) in flight (counts[nq], ids)
+	net( uint64_t n,
+	     uint64_t width,
+	     int const * edges,
+	     void * const * neuron_attrs,
+	     void * const * synapse_attrs,
+	     float dt,
+	     int delay,
+	     uint64_t step0,
+	     int nq,
+	     uint32_t const * counts,
+	     int const * ids )
+	    : impl( spice::util::layout( n, 0.0f ), dt, delay )
+	{
+		auto & base = static_cast<spice::snn<Model> &>( impl );
+		base.*member_pointer( istep_tag<Model>{} ) = static_cast<int>( step0 );
+		auto & clock = base.*member_pointer( simtime_tag<Model>{} );
+		for( uint64_t k = 0; k < step0; k++ ) clock.add( dt );
+		auto & spikes = impl.*member_pointer( spikes_tag<Model>{} );
+		size_t o = 0;
+		for( int q = 0; q < nq; q++ )
+		{
+			spikes.counts.push_back( counts[q] );
+			spikes.ids.insert( spikes.ids.end(), ids + o, ids + o + counts[q] );
+			// Brunel+ keeps each step's firing flags in slot step % (delay + 1)
+			if( spikes.flags )
+				for( uint32_t k = 0; k < counts[q]; k++ )
+					( *spikes.flags )[( step0 - nq + q ) % ( delay + 1 )][ids[o + k]] = true;
+			o += counts[q];
+		}
+		auto & graph = impl.*member_pointer( graph_tag<Model>{} );
+		graph.edges.assign( edges, edges + n * width );
+		graph.adj = spice::util::adj_list( n, width, graph.edges.data() );
+		if constexpr( Model::neuron::size > 0 )
+		{
+			auto & nv = *( impl.*member_pointer( neurons_tag<Model>{} ) );
+			using T = typename Model::neuron::tuple_t;
+			gather_tuple( nv, neuron_attrs, std::make_index_sequence<std::tuple_size_v<T>>() );
+		}
+		if constexpr( Model::synapse::size > 0 )
+		{
+			auto & sv = impl.*member_pointer( synapses_tag<Model>{} );
+			sv.emplace( n * width );
+			using T = typename Model::synapse::tuple_t;
+			gather_tuple( *sv, synapse_attrs, std::make_index_sequence<std::tuple_size_v<T>>() );
+		}
 	}
 
 	int step( int * out, int cap ) override
@@ -189,6 +307,55 @@ void * ref_create(
 		case 1: return new net<spice::brunel>( l, dt, delay );
 		case 2: return new net<spice::brunel_with_plasticity>( l, dt, delay );
 		case 3: return new net<spice::synth>( l, dt, delay );
+		default: g_err = "invalid model"; return nullptr;
+		}
+	}
+	catch( std::exception const & e )
+	{
+		g_err = e.what();
+		return nullptr;
+	}
+}
+
+// A reference net over an imported graph and state (see net's second constructor): the
+// graph n x width (rows ascending, INT_MAX padded, as adj() returns it), neuron_attrs one
+// array per neuron attribute and, for brunel_with_plasticity, synapse_attrs (W, Zpre,
+// Zpost) over all n x width slots. The Poisson stream restarts at step 0 with rng_seed.
+// With step0 > 0 the net continues a run at step step0 (clock, Poisson stream and the nq
+// steps of spikes in flight, counts[nq] and ids concatenated, oldest first); nq <= delay.
+void * ref_create_from_state(
+    int model,
+    uint64_t n,
+    uint64_t width,
+    int const * edges,
+    void * const * neuron_attrs,
+    void * const * synapse_attrs,
+    float dt,
+    int delay,
+    uint64_t rng_seed,
+    uint64_t step0,
+    int nq,
+    uint32_t const * counts,
+    int const * ids )
+{
+	try
+	{
+		if( nq < 0 || nq > delay || (uint64_t)nq > step0 ) throw std::invalid_argument( "spikes in flight: at most delay steps, none before step 0" );
+		oracle::counter_rng::seed = rng_seed;
+		oracle::counter_rng::npoisson = ( model == 3 ) ? n : ( n / 2 > 0 ? n / 2 : 1 );
+		oracle::counter_rng::calls = step0 * oracle::counter_rng::npoisson;
+		g_generate_calls++;
+		auto const a = std::make_tuple( n, width, edges, neuron_attrs, synapse_attrs, dt, delay, step0, nq, counts, ids );
+		auto make = [&]( auto tag ) -> net_base * {
+			using M = typename decltype( tag )::type;
+			return std::apply( []( auto... x ) { return new net<M>( x... ); }, a );
+		};
+		switch( model )
+		{
+		case 0: return make( std::common_type<spice::vogels_abbott>{} );
+		case 1: return make( std::common_type<spice::brunel>{} );
+		case 2: return make( std::common_type<spice::brunel_with_plasticity>{} );
+		case 3: return make( std::common_type<spice::synth>{} );
 		default: g_err = "invalid model"; return nullptr;
 		}
 	}

@@ -23,17 +23,28 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <memory>
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace oracle
 {
+// threads of the Brunel+ synapse sweep on large nets (ORACLE_THREADS, else the host's)
+static int sweep_threads()
+{
+	char const * e = std::getenv( "ORACLE_THREADS" );
+	int const t = e ? std::atoi( e ) : (int)std::thread::hardware_concurrency();
+	return std::max( 1, std::min( t, 64 ) );
+}
+
 // ---------------------------------------------------------------------------------------
 // layout  (spice/util/layout.cpp:51-110, estimate_max_deg :13-38)
 // ---------------------------------------------------------------------------------------
@@ -494,13 +505,28 @@ struct sim
 		queue.push_back( out );
 
 		if( s.model == BRUNEL_PLUS )
-			for( int src = 0; src < n; src++ )
-				for( int j = 0; j < row_len[src]; j++ )
-				{
-					int const dst = edges[(size_t)src * width + j];
-					if( plastic( src, dst, n ) )
-						stdp( (size_t)src * width + j, flags[pre][src], flags[post][dst], dt_ );
-				}
+		{
+			// every synapse's update reads only its own state and the step's flags, so rows
+			// are independent: large nets sweep them on several threads (same results)
+			auto sweep = [&]( int r0, int r1 ) {
+				for( int src = r0; src < r1; src++ )
+					for( int j = 0; j < row_len[src]; j++ )
+					{
+						int const dst = edges[(size_t)src * width + j];
+						if( plastic( src, dst, n ) ) stdp( (size_t)src * width + j, flags[pre][src], flags[post][dst], dt_ );
+					}
+			};
+			int const nthreads = (size_t)n * width < ( 1u << 22 ) ? 1 : sweep_threads();
+			if( nthreads <= 1 )
+				sweep( 0, n );
+			else
+			{
+				std::vector<std::thread> pool;
+				for( int k = 0; k < nthreads; k++ )
+					pool.emplace_back( sweep, (int)( (long long)n * k / nthreads ), (int)( (long long)n * ( k + 1 ) / nthreads ) );
+				for( auto & t : pool ) t.join();
+			}
+		}
 		istep++;
 	}
 };
@@ -749,6 +775,69 @@ void oracle_synapses( void * h, double ** a )
 		go( S<double>( h ) );
 	else
 		go( S<float>( h ) );
+}
+
+// Replace the neuron state (one array per attribute in the reference's order, float32 or
+// int32 as the model declares them) and, for Brunel+, the synapse state (W, Zpre, Zpost,
+// float32 over all n x width slots): a net that starts from another simulator's state, as
+// the conversion constructor does (spice/cuda/snn.d.cpp:201-221).
+void oracle_set_state( void * h, void * const * neurons, void * const * synapses )
+{
+	auto go = [&]( auto & s ) {
+		using R = typename std::remove_reference_t<decltype( s.s.V )>::value_type;
+		auto fl = [&]( auto & dst, void const * src ) {
+			float const * f = static_cast<float const *>( src );
+			for( size_t i = 0; i < dst.size(); i++ ) dst[i] = static_cast<R>( f[i] );
+		};
+		auto in = [&]( std::vector<int> & dst, void const * src ) { std::memcpy( dst.data(), src, dst.size() * 4 ); };
+		switch( s.s.model )
+		{
+		case VOGELS_ABBOTT: fl( s.s.V, neurons[0] ), fl( s.s.Gex, neurons[1] ), fl( s.s.Gin, neurons[2] ), in( s.s.Twait, neurons[3] ); break;
+		case BRUNEL:
+		case BRUNEL_PLUS: fl( s.s.V, neurons[0] ), in( s.s.Twait, neurons[1] ); break;
+		case SYNTH: in( s.s.Ncount, neurons[0] ); break;
+		}
+		if( s.s.model == BRUNEL_PLUS && synapses ) fl( s.s.W, synapses[0] ), fl( s.s.Zpre, synapses[1] ), fl( s.s.Zpost, synapses[2] );
+	};
+	if( is64( h ) )
+		go( S<double>( h ) );
+	else
+		go( S<float>( h ) );
+}
+
+// Continue a run at step step0: the simulated clock advanced by step0 steps (the Poisson
+// draws keyed by the step follow) and the spikes of the steps [step0 - nq, step0) in flight
+// (counts[nq], ids concatenated, oldest first; nq <= delay), with their firing flags.
+int oracle_set_progress( void * h, uint64_t step0, int nq, uint32_t const * counts, int const * ids )
+{
+	auto go = [&]( auto & s ) {
+		if( nq < 0 || nq > s.delay || (uint64_t)nq > step0 ) throw std::invalid_argument( "spikes in flight: at most delay steps" );
+		s.istep = (int)step0;
+		s.clock = kahan{};
+		for( uint64_t k = 0; k < step0; k++ ) s.clock.add( s.dt );
+		s.queue.clear();
+		size_t o = 0;
+		for( int q = 0; q < nq; q++ )
+		{
+			s.queue.emplace_back( ids + o, ids + o + counts[q] );
+			if( s.s.model == BRUNEL_PLUS )
+				for( uint32_t k = 0; k < counts[q]; k++ ) s.flags[( step0 - nq + q ) % ( s.delay + 1 )][ids[o + k]] = 1;
+			o += counts[q];
+		}
+	};
+	try
+	{
+		if( is64( h ) )
+			go( S<double>( h ) );
+		else
+			go( S<float>( h ) );
+		return 0;
+	}
+	catch( std::exception const & e )
+	{
+		g_err = e.what();
+		return -1;
+	}
 }
 
 // Exact float32 views for bit-level comparisons (precision 32 only).

@@ -1161,6 +1161,30 @@ void enqueue_generate( cudaStream_t s, spice::util::layout const & l, unsigned l
 	CK( cudaGetLastError() );
 }
 
+// ELL rows as the reference keeps them (spice/util/adj_list.cpp:28-46): every row strictly
+// ascending, every target in [0, n), INT_MAX padding only at the end of a row. The
+// pivot and slice builders rely on it, so imported graphs are checked on the host first.
+void validate_edges( int32_t const * edges, uint64_t n, uint64_t width )
+{
+	for( uint64_t i = 0; i < n; i++ )
+	{
+		int prev = -1;
+		bool pad = false;
+		for( uint64_t j = 0; j < width; j++ )
+		{
+			int const v = edges[i * width + j];
+			if( v == INT_MAX )
+			{
+				pad = true;
+				continue;
+			}
+			require( !pad, "edges: padding must end a row" );
+			require( v > prev && (uint64_t)v < n, "edges: rows must be strictly ascending and in range" );
+			prev = v;
+		}
+	}
+}
+
 // Upper estimate of the device memory a net of this layout holds once built (the buffers
 // of allocate, build_slices and the plastic state; slices bounded by one 16-byte vector per
 // 8 or 12 synapses plus one per non-empty (source, tile) pair, at 5 % above the expected
@@ -1271,6 +1295,133 @@ std::vector<std::pair<uint32_t, spk::plastic_state::buf *>> ckpt_plastic( spk_ne
 	return { { 40, &q.W },        { 41, &q.za },         { 42, &q.zpre },       { 43, &q.zpost },     { 44, &q.hist },
 	         { 45, &q.rf_a },     { 46, &q.zrf_a },      { 47, &q.rf_c },       { 48, &q.zrf_c },     { 49, &q.ring_meta },
 	         { 50, &q.flush_ring }, { 51, &q.flush_cnt }, { 52, &q.ring_pot } };
+}
+
+// The contents a restored net's kernels index with, checked on the host before any
+// device work: the edges (as an imported graph), the tiling and kernel shape against
+// what the builders can produce, the spike ring's per-tile segments and, for Brunel+,
+// the lazy-STDP rings and row states. A corrupted or hand-edited checkpoint is refused
+// with SPK_ERR_INVALID instead of sending a kernel outside its buffers.
+using ckpt_dir = std::vector<std::tuple<uint32_t, uint64_t, unsigned char const *>>;
+unsigned char const * ckpt_find( ckpt_dir const & dir, uint32_t id, uint64_t bytes )
+{
+	for( auto const & d : dir )
+		if( std::get<0>( d ) == id )
+		{
+			require( std::get<1>( d ) == bytes, "checkpoint buffer size differs from the net's" );
+			return std::get<2>( d );
+		}
+	throw spk_error( SPK_ERR_INVALID, "checkpoint lacks a buffer" );
+}
+template <typename T>
+std::vector<T> ckpt_read( ckpt_dir const & dir, uint32_t id, uint64_t count )
+{
+	std::vector<T> v( count );
+	if( count ) std::memcpy( v.data(), ckpt_find( dir, id, count * sizeof( T ) ), count * sizeof( T ) );
+	return v;
+}
+void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first, ckpt_dir const & dir )
+{
+	uint64_t const n = (uint64_t)h.n, width = (uint64_t)h.width;
+	int const T = h.ntiles;
+	bool const plastic = h.model == SPK_BRUNEL_PLUS;
+	// the graph
+	int32_t const * edges = n * width ? reinterpret_cast<int32_t const *>( ckpt_find( dir, 1, n * width * 4 ) ) : nullptr;
+	if( edges )
+	{
+		// read in place when aligned (the directory keeps buffers at 4-byte offsets)
+		std::vector<int32_t> copy;
+		int32_t const * e = edges;
+		if( reinterpret_cast<uintptr_t>( edges ) % alignof( int32_t ) )
+		{
+			copy.resize( n * width );
+			std::memcpy( copy.data(), edges, n * width * 4 );
+			e = copy.data();
+		}
+		validate_edges( e, n, width );
+		// tiles that receive synapses
+		std::vector<char> in_tile( T, 0 );
+		std::vector<char> target( n, 0 );
+		for( uint64_t k = 0; k < n * width; k++ )
+			if( e[k] != INT_MAX ) target[e[k]] = 1;
+		for( int j = 0; j < T; j++ )
+			for( int d = first[j]; d < first[j + 1] && !in_tile[j]; d++ ) in_tile[j] = target[d];
+		if( h.flat )
+		{
+			unsigned const pad = h.pack == 12 ? spk::SLICE_PAD10 : spk::SLICE_PAD;
+			for( int j = 0; j < T; j++ )
+				if( in_tile[j] )
+				{
+					long long const span = first[j + 1] - first[j];
+					require( span <= h.flat_tmax && (long long)classes_of( h.model ) * span < (long long)pad,
+					         "checkpoint tiling does not fit its kernel: a tile with inputs exceeds the tile limit" );
+				}
+		}
+	}
+	// the kernel shape
+	if( h.flat )
+	{
+		require( !plastic && T + 1 < spk::FLAT_PC && h.threads == spk::FLAT_THREADS && h.npt == 1 && h.tile == h.flat_tmax &&
+		             h.flat_tmax >= 32 && h.flat_tmax <= spk::FLAT_MAX_TILE && h.flat_tmax % 32 == 0,
+		         "checkpoint tiling does not fit its kernel" );
+	}
+	else
+	{
+		require( ( h.npt == 1 || h.npt == 2 || h.npt == 4 ) && h.threads >= 32 && h.threads <= 512 && h.threads % 32 == 0 &&
+		             h.tile == h.threads * h.npt && h.tile <= ( plastic ? 512 : 2048 ) && first == uniform_tiles( h.n, h.tile ),
+		         "checkpoint tiling does not fit its kernel" );
+	}
+	// the spike ring: per slot and tile, an ascending run of the tile's own neurons
+	uint64_t const slots = (uint64_t)h.ring_slots;
+	auto const cnt = ckpt_read<uint32_t>( dir, 21, slots * T );
+	auto const ids = ckpt_read<int32_t>( dir, 20, slots * n );
+	auto check_segments = [&]( std::vector<uint32_t> const & counts, auto && id_at, char const * what ) {
+		for( uint64_t sl = 0; sl < counts.size() / T; sl++ )
+			for( int j = 0; j < T; j++ )
+			{
+				uint32_t const c = counts[sl * T + j];
+				require( c <= (uint32_t)( first[j + 1] - first[j] ), what );
+				int prev = first[j] - 1;
+				for( uint32_t k = 0; k < c; k++ )
+				{
+					int const v = id_at( sl * n + first[j] + k );
+					require( v > prev && v < first[j + 1], what );
+					prev = v;
+				}
+			}
+	};
+	check_segments( cnt, [&]( uint64_t i ) { return ids[i]; }, "checkpoint spike ring is inconsistent" );
+	if( !plastic ) return;
+	// Brunel+: the flush ring's sources and every replay window at most the history's 64
+	// steps; row states pending no longer than the forced flush allows
+	struct ent
+	{
+		int32_t a, b, c, d;
+	};
+	uint64_t const ps = 2ull * h.delay;
+	require( slots == ps, "checkpoint spike ring is inconsistent" );
+	auto const fcnt = ckpt_read<uint32_t>( dir, 51, ps * T );
+	auto const fring = ckpt_read<ent>( dir, 50, ps * n );
+	auto const meta = ckpt_read<ent>( dir, 49, ps * n );
+	check_segments( fcnt, [&]( uint64_t i ) { return fring[i].a; }, "checkpoint flush ring is inconsistent" );
+	for( uint64_t sl = 0; sl < ps; sl++ )
+		for( int j = 0; j < T; j++ )
+		{
+			for( uint32_t k = 0; k < fcnt[sl * T + j]; k++ )
+				require( fring[sl * n + first[j] + k].b >= 0 && fring[sl * n + first[j] + k].b <= 64, "checkpoint flush ring is inconsistent" );
+			for( uint32_t k = 0; k < cnt[sl * T + j]; k++ )
+				require( ( meta[sl * n + first[j] + k].a & 0xff ) <= 64, "checkpoint spike ring is inconsistent" );
+		}
+	long long const now = (long long)h.steps;
+	auto const rf_a = ckpt_read<int32_t>( dir, 45, n );
+	auto const rf_c = ckpt_read<int32_t>( dir, 47, n );
+	for( uint64_t i = 0; i < n; i++ )
+	{
+		require( rf_a[i] == -1 || ( rf_a[i] >= 0 && rf_a[i] >= now + h.delay - 64 && rf_a[i] <= now + h.delay ),
+		         "checkpoint STDP row state is inconsistent" );
+		require( rf_c[i] == -1 || ( rf_c[i] >= 0 && rf_c[i] >= now - 64 && rf_c[i] <= now + h.delay ),
+		         "checkpoint STDP row state is inconsistent" );
+	}
 }
 
 // pooled: the net's buffers come from the device's stream-ordered pool and its stream
@@ -1659,24 +1810,7 @@ int spk_net_create_from_adj(
 		require( edges != nullptr || num_neurons * width == 0, "edges is null" );
 		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device ) );
 		device_guard g( device );
-		// validate rows: ascending, in range, INT_MAX padded
-		for( uint64_t i = 0; i < num_neurons; i++ )
-		{
-			int prev = -1;
-			bool pad = false;
-			for( uint64_t j = 0; j < width; j++ )
-			{
-				int const v = edges[i * width + j];
-				if( v == INT_MAX )
-				{
-					pad = true;
-					continue;
-				}
-				require( !pad, "edges: padding must end a row" );
-				require( v > prev && (uint64_t)v < num_neurons, "edges: rows must be strictly ascending and in range" );
-				prev = v;
-			}
-		}
+		validate_edges( edges, num_neurons, width );
 		allocate( *net, (long long)num_neurons, (long long)width, adjacency_costs( edges, (long long)num_neurons, (long long)width ) );
 		if( num_neurons * width )
 			CK( cudaMemcpyAsync( net->edges.p, edges, num_neurons * width * 4, cudaMemcpyHostToDevice, net->stream ) );
@@ -1984,8 +2118,8 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		in += tiles_bytes;
 		require( first[0] == 0 && first[h.ntiles] == h.n, "checkpoint tiling is inconsistent" );
 		for( int i = 0; i < h.ntiles; i++ ) require( first[i] < first[i + 1], "checkpoint tiling is inconsistent" );
-		// read the buffer directory first: every size checked before any device work
-		std::vector<std::tuple<uint32_t, uint64_t, unsigned char const *>> dir;
+		// read the buffer directory first: every size and index checked before any device work
+		ckpt_dir dir;
 		unsigned char const * end = static_cast<unsigned char const *>( buf ) + size;
 		for( int b = 0; b < h.nbufs; b++ )
 		{
@@ -1999,6 +2133,7 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 			dir.emplace_back( id, bytes, in );
 			in += bytes;
 		}
+		validate_checkpoint( h, first, dir );
 
 		std::unique_ptr<spk_net> net( new_net( h.model, h.dt, h.delay, h.seed, device ) );
 		device_guard g( device );
@@ -2012,15 +2147,13 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		set_tiles( *net, first );
 		net->ring_slots = h.ring_slots;
 		allocate_buffers( *net );
-		auto find = [&]( uint32_t id, uint64_t bytes ) -> unsigned char const * {
-			for( auto const & d : dir )
-				if( std::get<0>( d ) == id )
-				{
-					require( std::get<1>( d ) == bytes, "checkpoint buffer size differs from the net's" );
-					return std::get<2>( d );
-				}
-			throw spk_error( SPK_ERR_INVALID, "checkpoint lacks a buffer" );
-		};
+		auto find = [&]( uint32_t id, uint64_t bytes ) { return ckpt_find( dir, id, bytes ); };
+		// tiles without inputs keep only their state in shared memory: it must fit the
+		// window kernel's shared memory (configured by allocate_buffers)
+		if( net->flat )
+			for( int j = 0; j < h.ntiles; j++ )
+				require( spk::flat_state_bytes( net->neuron_attrs(), first[j + 1] - first[j] ) <= (size_t)net->flat_smem,
+				         "checkpoint tiling does not fit its kernel: a tile exceeds the shared memory" );
 		// edges first: the pivots and slices are rebuilt from them (which resets the
 		// publication flags), then the state over them
 		dbuf & e = net->edges;
@@ -2068,8 +2201,11 @@ int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs,
 // has already budgeted and can fail at an arbitrary point), and latency-critical loops
 // that cannot afford the device-wide synchronisation cudaMalloc / cudaFree imply. For
 // them this variant keeps the generator's connection table in a fixed device array of
-// this file instead of a fresh allocation; the host side flattens the layout in stack
-// arrays only.
+// this file instead of a fresh allocation. The host side flattens the layout in
+// per-thread static arrays (no heap, about 36 KiB kept off the caller's stack), and the
+// table reaches the device array through kernel parameters: each launch of
+// store_static_conns carries its own copy of up to STATIC_CHUNK connections, so nothing
+// on the device side ever refers to host memory of the call.
 // ---------------------------------------------------------------------------------------
 namespace
 {
@@ -2083,6 +2219,19 @@ __device__ __align__( 256 ) spk::conn_dev g_static_conns[STATIC_MAX_CONNECTIONS]
 constexpr int MAX_DEVICES = 64;
 void * g_static_conns_ptr[MAX_DEVICES] = {};
 std::mutex g_static_mutex;
+
+// a piece of the connection table, passed by value as a kernel parameter (3 KiB, inside
+// the 4 KiB parameter space of every launch)
+constexpr int STATIC_CHUNK = 128;
+struct static_chunk
+{
+	spk::conn_dev c[STATIC_CHUNK];
+};
+__global__ void store_static_conns( static_chunk chunk, int offset, int count, spk::conn_dev * dst )
+{
+	int const i = threadIdx.x;
+	if( i < count ) dst[offset + i] = chunk.c[i];
+}
 
 void * static_conns_address( int device )
 {
@@ -2107,8 +2256,10 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 		require( d->nconn >= 0 && d->nconn <= STATIC_MAX_CONNECTIONS, "spk_generate_adj_list_static: at most 1024 connections" );
 		require( d->nconn == 0 || ( d->conn_src && d->conn_dst && d->conn_p ), "bad connection arrays" );
 
-		// the layout, flattened exactly as spice::util::layout does, in stack arrays
-		unsigned long long first[STATIC_MAX_POPULATIONS + 1];
+		// the layout, flattened exactly as spice::util::layout does, in per-thread arrays
+		static thread_local unsigned long long first[STATIC_MAX_POPULATIONS + 1];
+		static thread_local int order[STATIC_MAX_CONNECTIONS];
+		static thread_local spk::conn_dev table[STATIC_MAX_CONNECTIONS];
 		first[0] = 0;
 		for( int i = 0; i < d->npops; i++ )
 		{
@@ -2116,7 +2267,6 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 			first[i + 1] = first[i] + d->pops[i];
 		}
 		require( first[d->npops] <= (unsigned long long)INT_MAX, "too many neurons" );
-		int order[STATIC_MAX_CONNECTIONS];
 		for( int i = 0; i < d->nconn; i++ )
 		{
 			require( d->conn_src[i] >= 0 && d->conn_src[i] < d->npops && d->conn_dst[i] >= 0 && d->conn_dst[i] < d->npops,
@@ -2132,7 +2282,6 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 		for( int i = 1; i < d->nconn; i++ )
 			require( less( order[i - 1], order[i] ), "no duplicate edges in connections list allowed" );
 
-		spk::conn_dev table[STATIC_MAX_CONNECTIONS];
 		for( int i = 0; i < d->nconn; i++ )
 		{
 			int const c = order[i], s = d->conn_src[c], t = d->conn_dst[c];
@@ -2164,13 +2313,18 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 		CK( cudaGetDevice( &device ) );
 		void * conns = static_conns_address( device );
 		cudaStream_t const s = static_cast<cudaStream_t>( stream );
-		if( d->nconn )
-			CK( cudaMemcpyAsync( conns, table, (size_t)d->nconn * sizeof( spk::conn_dev ), cudaMemcpyHostToDevice, s ) );
+		// the table in pieces of STATIC_CHUNK connections, each launch holding its own copy
+		for( int o = 0; o < d->nconn; o += STATIC_CHUNK )
+		{
+			static_chunk chunk{};
+			int const count = std::min( STATIC_CHUNK, d->nconn - o );
+			std::memcpy( chunk.c, table + o, (size_t)count * sizeof( spk::conn_dev ) );
+			store_static_conns<<<1, STATIC_CHUNK, 0, s>>>( chunk, o, count, static_cast<spk::conn_dev *>( conns ) );
+			CK( cudaGetLastError() );
+		}
 		int const blocks = (int)( ( n * 32 + 255 ) / 256 );
 		spk::generate_ell<<<blocks, 256, 0, s>>>( (int)n, (int)w, d->nconn, static_cast<spk::conn_dev const *>( conns ), seed, d_edges );
 		CK( cudaGetLastError() );
-		// cudaMemcpyAsync from pageable memory returns once the source has been staged, so
-		// the stack table may go out of scope while the copy and the kernel are in flight
 	} );
 }
 

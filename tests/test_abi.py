@@ -100,3 +100,64 @@ def test_restore_rejects_bad_checkpoints_before_device_work(lib):
     assert lib.spk_net_restore(C.byref(h), junk, 8, 0) == spice_b200.ERR_INVALID
     assert b"truncated" in lib.spk_last_error()
     assert lib.spk_net_checkpoint(None, None, 0, None) == spice_b200.ERR_INVALID
+
+
+def _checkpoint_bytes(edges, n, width, ring_cnt=None, ring_ids=None, threads=64, tile=64, model=1, delay=2):
+    """A checkpoint laid out as spk_net_checkpoint writes it (header, tile starts, then
+    {u32 id, u64 bytes, data} per buffer) for a one-tile Brunel net."""
+    import struct
+
+    import numpy as np
+
+    slots = 2 * delay
+    ntiles = (n + tile - 1) // tile
+    first = np.array([min(j * tile, n) for j in range(ntiles + 1)], np.int32)
+    bufs = [(1, np.asarray(edges, np.int32).tobytes())]
+    bufs += [(10, np.zeros(n, np.float32).tobytes()), (11, np.zeros(n, np.int32).tobytes())]
+    ids = np.zeros(slots * n, np.int32) if ring_ids is None else np.asarray(ring_ids, np.int32)
+    cnt = np.zeros(slots * ntiles, np.uint32) if ring_cnt is None else np.asarray(ring_cnt, np.uint32)
+    bufs += [(20, ids.tobytes()), (21, cnt.tobytes()), (22, bytes(24)), (23, bytes(512))]
+    head = struct.pack("<8sIiqqifQQ8i2i", b"SPKCKPT1", 1, model, n, width, delay, 1e-4, 1, 0,
+                       ntiles, 0, 8, slots, 0, threads, 1, tile, len(bufs), 0)
+    assert len(head) == 96
+    out = head + first.tobytes()
+    for i, b in bufs:
+        out += struct.pack("<IQ", i, len(b)) + b
+    return out
+
+
+def test_restore_checks_contents_before_device_work(lib):
+    """Corrupted edges, tilings a kernel cannot run and spike-ring entries outside their tile
+    are refused with SPK_ERR_INVALID before the restore touches a device."""
+    import ctypes as C
+
+    import numpy as np
+
+    n, width = 64, 32
+    edges = np.full((n, width), np.iinfo(np.int32).max, np.int32)
+    edges[:, 0], edges[:, 1] = 5, 9
+
+    def restore(data):
+        h = C.c_void_p()
+        buf = (C.c_ubyte * len(data)).from_buffer_copy(data)
+        return lib.spk_net_restore(C.byref(h), buf, len(data), 0), lib.spk_last_error()
+
+    bad = edges.copy()
+    bad[3, :2] = [9, 5]  # descending row
+    rc, msg = restore(_checkpoint_bytes(bad, n, width))
+    assert rc == spice_b200.ERR_INVALID and b"edges" in msg
+    bad = edges.copy()
+    bad[7, 1] = n  # target out of range
+    rc, msg = restore(_checkpoint_bytes(bad, n, width))
+    assert rc == spice_b200.ERR_INVALID and b"edges" in msg
+    rc, msg = restore(_checkpoint_bytes(edges, n, width, threads=48, tile=48))  # not a multiple of 32
+    assert rc == spice_b200.ERR_INVALID and b"tiling" in msg
+    cnt = np.zeros(4, np.uint32)
+    cnt[1] = 65  # more spikes than the tile has neurons
+    rc, msg = restore(_checkpoint_bytes(edges, n, width, ring_cnt=cnt))
+    assert rc == spice_b200.ERR_INVALID and b"spike ring" in msg
+    cnt[1] = 2
+    ids = np.zeros(4 * n, np.int32)
+    ids[n:n + 2] = [3, 3]  # not ascending
+    rc, msg = restore(_checkpoint_bytes(edges, n, width, ring_cnt=cnt, ring_ids=ids))
+    assert rc == spice_b200.ERR_INVALID and b"spike ring" in msg

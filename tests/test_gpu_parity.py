@@ -529,3 +529,68 @@ def test_zero_steps_and_small_output_buffers():
     with pytest.raises(spice_b200.CapacityError):
         net.run_record(50, cap=1)  # Poisson neurons alone fire more than one spike in 50 steps
     assert net.info().steps == 150  # the state advanced; nothing was copied
+
+
+def _ckpt_dir(data):
+    """Header fields and {buffer id: (offset, bytes)} of checkpoint bytes."""
+    import struct
+
+    h = list(struct.unpack_from("<8sIiqqifQQ8i2i", data, 0))
+    off = 96 + 4 * (h[9] + 1)
+    d = {}
+    for _ in range(h[17]):
+        i, b = struct.unpack_from("<IQ", data, off)
+        off += 12
+        d[i] = (off, b)
+        off += b
+    return h, d
+
+
+def _patched(data, offset, dtype, value):
+    buf = bytearray(data)
+    buf[offset:offset + np.dtype(dtype).itemsize] = np.array([value], dtype).tobytes()
+    return bytes(buf)
+
+
+def test_restore_refuses_corrupted_checkpoints():
+    """Checkpoints of real nets with one corrupted entry (an edge, the tile limit, a spike
+    id, an STDP row state) are refused with SPK_ERR_INVALID; the intact ones restore."""
+    import struct
+
+    a = Snn("brunel", Layout([20_000, 20_000], [(0, 1, 0.05), (1, 1, 0.05)]), delay=15, seed=9, graph_seed=9)
+    a.run(80)
+    data = a.checkpoint()
+    h, d = _ckpt_dir(data)
+    assert h[10] == 1  # flat tiling
+    eoff, _ = d[1]
+    row0 = np.frombuffer(data, np.int32, count=int(h[4]), offset=eoff)
+    bad = _patched(data, eoff + 4, np.int32, int(row0[0]))  # repeated target: not ascending
+    with pytest.raises(spice_b200.InvalidArgument, match="edges"):
+        Snn.restore(bad)
+    hb = bytearray(data)
+    struct.pack_into("<ii", hb, 56 + 4 * 4, 64, 1024)  # flat_tmax, threads
+    struct.pack_into("<i", hb, 56 + 7 * 4, 64)         # tile
+    with pytest.raises(spice_b200.InvalidArgument, match="tiling"):
+        Snn.restore(bytes(hb))
+    coff, cb = d[21]
+    cnt = np.frombuffer(data, np.uint32, count=cb // 4, offset=coff)
+    k = int(np.flatnonzero(cnt)[0])
+    slot, tile = divmod(k, h[9])
+    first = np.frombuffer(data, np.int32, count=h[9] + 1, offset=96)
+    ioff, _ = d[20]
+    bad = _patched(data, ioff + 4 * (slot * h[3] + int(first[tile])), np.int32, int(first[tile + 1]))
+    with pytest.raises(spice_b200.InvalidArgument, match="spike ring"):
+        Snn.restore(bad)
+    b = Snn.restore(data)
+    assert np.array_equal(a.step(out=True), b.step(out=True))
+
+    p = Snn("brunel_with_plasticity", Layout([1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15, seed=9, graph_seed=9)
+    p.run(150)
+    data = p.checkpoint()
+    h, d = _ckpt_dir(data)
+    roff, _ = d[45]
+    bad = _patched(data, roff + 4 * 1500, np.int32, 0)  # a pending row state older than the history
+    with pytest.raises(spice_b200.InvalidArgument, match="STDP"):
+        Snn.restore(bad)
+    q = Snn.restore(data)
+    assert np.array_equal(p.step(out=True), q.step(out=True))
