@@ -30,7 +30,6 @@ CONNS = [(0, 1, 0.1), (1, 1, 0.1)]
 DT, DELAY = 1e-4, 15
 SIM_STEPS = 1050                      # per bench step
 METRIC = "wall/bio time ratio at 1e9-syn Brunel"
-CPU_SAMPLE_STEPS = 120                # reference CPU sample (about 10-30 s on one core)
 
 
 def parse():
@@ -143,9 +142,12 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
+def profile_traffic(syn):
     """DRAM bytes per simulated step of the window kernel from the committed ncu summary
-    (bytes per captured launch / steps per captured launch), if any."""
+    (bytes per captured launch / steps per captured launch), for the size it was captured
+    at (1e9 synapses) only."""
+    if syn != 1e9:
+        return None
     path = os.path.join(ROOT, "profiles", "window_flat_brunel_1e9.json")
     try:
         with open(path) as f:
@@ -155,65 +157,110 @@ def profile_traffic():
         return None
 
 
-def cpu_baseline():
+L2_BYTES = 126e6
+
+
+def net_config(syn, width, world):
+    """The workload both arms run: the same keys in the GPU and the reference line."""
+    n = sum(POPS)
+    table = n * width * 4
+    l2 = (f"inputs larger than L2 ({table / 1e9:.2f} GB synapse table)" if table > L2_BYTES
+          else f"synapse table ({table / 1e6:.0f} MB) fits L2: no flush between steps")
+    return {"workload": f"brunel_{syn:.0e}".replace("+0", ""), "neurons": n, "synapses": syn, "ell_width": width,
+            "dt": DT, "delay": DELAY, "model": "brunel", "parallelism": f"replicas{world}", "l2": l2}
+
+
+# CPU steps timed per sample: the reference's cpu::snn takes about 0.065 s per step of the
+# 1e9 net at steady state on one core
+CPU_SAMPLE_STEPS = 135
+CPU_WARM_STEPS = 600  # reference arm: the activity settles within about 300 steps
+
+
+def cpu_baseline(net):
     """The reference's cpu::snn (oracle/_ref, built with the reference's own -O2 -ffast-math)
-    on the same Brunel 1e9 net, one core, a bounded sample of steps after the first `delay`
-    steps (when the spike queue is full). Falls back to the CPU restatement (kind "port")
-    where the reference build is absent. Returns (wall/bio, kind, cores, sample text)."""
-    t0 = time.perf_counter()
-    net, kind = make_cpu_net()
-    setup = time.perf_counter() - t0
-    for _ in range(DELAY):
-        net.step()
+    continuing the GPU net at its steady state: the GPU net's last `delay` steps are
+    recorded and its graph and state handed to the reference (same clock, Poisson stream and
+    spikes in flight), then both advance CPU_SAMPLE_STEPS steps. The reference's time on one
+    core is the baseline; its raster and final state, compared with the GPU's, are the
+    parity flag. Falls back to the CPU restatement (kind "port") where the reference build
+    is absent. Returns (wall/bio, kind, cores, sample text, parity, spikes per step)."""
+    import oracle
+
+    counts, ids = net.run_record(DELAY)
+    step0 = net.info().steps
+    edges, width = net.adj()
+    neurons = net.neurons()
+    if oracle.have_reference(fast=True):
+        cpu = oracle.ReferenceNet.from_state("brunel", edges, width, neurons, dt=DT, delay=DELAY, seed=1, fast=True,
+                                             step0=step0, counts=counts, ids=ids)
+        kind = "reference"
+    else:
+        cpu = oracle.OracleNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, edges=edges, width=width)
+        cpu.set_state(neurons)
+        cpu.set_progress(step0, counts, ids)
+        kind = "port"
+    del edges
+    gc, gi = net.run_record(CPU_SAMPLE_STEPS)
+    off = np.concatenate([[0], np.cumsum(gc)]).astype(np.int64)
+    parity = True
     t0 = time.perf_counter()
     spikes = 0
-    for _ in range(CPU_SAMPLE_STEPS):
-        spikes += len(net.step())
+    for k in range(CPU_SAMPLE_STEPS):
+        s = cpu.step()
+        spikes += len(s)
+        parity = parity and np.array_equal(s, gi[off[k]:off[k + 1]])
     wall = time.perf_counter() - t0
-    del net
+    for a, b in zip(net.neurons(), cpu.neurons()):
+        parity = parity and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    del cpu
     ratio = wall / (CPU_SAMPLE_STEPS * DT)
-    sample = (f"Brunel 1e9 (N=141,420, width 7,328), {CPU_SAMPLE_STEPS} steps after the first {DELAY} "
-              f"({CPU_SAMPLE_STEPS * DT * 1e3:.0f} ms biological, {spikes} spikes), single thread, setup {setup:.1f} s excluded")
-    return ratio, kind, 1, sample
+    sample = (f"Brunel {sum(POPS):,} neurons, {CPU_SAMPLE_STEPS} steps continuing the GPU net at steady state "
+              f"(steps {step0}-{step0 + CPU_SAMPLE_STEPS - 1}, {spikes / CPU_SAMPLE_STEPS:.0f} spikes per step), single thread, "
+              f"graph and state import excluded")
+    return ratio, kind, 1, sample, bool(parity), spikes / CPU_SAMPLE_STEPS
 
 
 REF_SIM_STEPS = 20  # simulation steps timed per reference-arm bench step
 
 
-def make_cpu_net():
-    import oracle
-
-    if oracle.have_reference(fast=True):
-        return oracle.ReferenceNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, fast=True), "reference"
-    return oracle.OracleNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, graph="reference", graph_seed=1337), "port"
-
-
 def run_reference(args, rank, world):
-    """The reference's CPU simulator on the same workload, rank 0 only: each bench step
-    times REF_SIM_STEPS steps of one constructed net (setup excluded, like the reference)."""
+    """The reference's CPU simulator on the same workload, rank 0 only: the reference's
+    cpu::snn builds the net from its own layout and generator, runs CPU_WARM_STEPS untimed
+    steps past the initial transient, then each bench step times REF_SIM_STEPS steps
+    (setup excluded, like the reference)."""
     if rank != 0:
         return
+    import oracle
+
     t0 = time.perf_counter()
-    net, kind = make_cpu_net()
+    if oracle.have_reference(fast=True):
+        net, kind = oracle.ReferenceNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, fast=True), "reference"
+    else:
+        net, kind = oracle.OracleNet("brunel", POPS, CONNS, dt=DT, delay=DELAY, seed=1, graph="reference",
+                                     graph_seed=1337), "port"
     setup = time.perf_counter() - t0
-    for _ in range(DELAY):
+    for _ in range(CPU_WARM_STEPS):
         net.step()
-    vals = []
+    vals, spikes = [], 0
     for i in range(args.warmup + args.steps):
         t = time.perf_counter()
         for _ in range(REF_SIM_STEPS):
-            net.step()
+            c = len(net.step())
+            if i >= args.warmup:
+                spikes += c
         if i >= args.warmup:
             vals.append((time.perf_counter() - t) / (REF_SIM_STEPS * DT))
     value = statistics.median(vals) if vals else None
-    sample = (f"Brunel 1e9 (N=141,420), {REF_SIM_STEPS} steps per bench step x {args.steps}, single thread "
-              f"(cpu::snn has no threading), setup {setup:.1f} s excluded")
+    first = CPU_WARM_STEPS + args.warmup * REF_SIM_STEPS
+    sps = spikes / max(1, args.steps * REF_SIM_STEPS)
+    sample = (f"Brunel {sum(POPS):,} neurons, {REF_SIM_STEPS} steps per bench step x {args.steps} (steps {first}-"
+              f"{first + args.steps * REF_SIM_STEPS - 1}, after {CPU_WARM_STEPS} steps past the initial transient; "
+              f"{sps:.0f} spikes per step), single thread (cpu::snn has no threading), setup {setup:.1f} s excluded")
     line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * REF_SIM_STEPS * DT * 1e3 if value else None,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": "brunel_1e9", "neurons": sum(POPS), "synapses": 1e9, "dt": DT, "delay": DELAY,
-                       "model": "brunel"},
+            "impl": "reference", "config": net_config(args.syn, int(net.width), world),
+            "sim_steps_per_bench_step": REF_SIM_STEPS, "spikes_per_step": sps,
             "cpu_baseline": {"value": value, "unit": "wall_s/bio_s", "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -269,7 +316,6 @@ def run_ours(args, rank, world):
         e2e_vals.append(time.perf_counter() - t)
         d2h.append(c.nbytes + ids.nbytes)
     e2e_wall = max_over_ranks(statistics.median(e2e_vals), world)
-    net.close()
 
     bio = args.steps * S * DT
     value = (ms_max / 1e3) / (bio * world)
@@ -287,17 +333,15 @@ def run_ours(args, rank, world):
     t_launch = (ms / 1e3) / launches
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / t_launch / 1e9
-    traffic_per_step = profile_traffic()
+    traffic_per_step = profile_traffic(args.syn)
     traffic = traffic_per_step * steps_per_launch if traffic_per_step else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "wall_s/bio_s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"brunel_{args.syn:.0e}".replace("+0", ""), "neurons": n, "synapses": args.syn, "ell_width": info.width,
-                           "dt": DT, "delay": DELAY, "model": "brunel", "sim_steps_per_bench_step": S,
-                           "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (4.15 GB synapse table)",
-                           "tiles": info.num_tiles, "tile_size": info.tile_size, "setup_s": setup_s,
-                           "spikes_per_step": spikes_per_step},
+                "config": net_config(args.syn, int(info.width), world),
+                "sim_steps_per_bench_step": S, "spikes_per_step": spikes_per_step, "setup_s": setup_s,
+                "tiles": info.num_tiles, "tile_size": info.tile_size,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "traffic": traffic, "peak_kind": peak_kind, "kernel": "window_flat<brunel>",
                              "bytes_per_launch": bytes_per_launch, "launch_us": t_launch * 1e6,
@@ -308,12 +352,15 @@ def run_ours(args, rank, world):
                 "gpu_launches": launches, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             try:
-                v, kind, cores, sample = cpu_baseline()
-                line["cpu_baseline"] = {"value": v, "unit": "wall_s/bio_s", "cores": cores, "kind": kind, "sample": sample}
+                v, kind, cores, sample, parity, cpu_sps = cpu_baseline(net)
+                line["cpu_baseline"] = {"value": v, "unit": "wall_s/bio_s", "cores": cores, "kind": kind, "sample": sample,
+                                        "spikes_per_step": cpu_sps}
+                line["parity"] = parity
             except Exception as e:  # report, never fail the GPU line
                 line["cpu_baseline"] = {"value": None, "unit": "wall_s/bio_s", "cores": 1, "kind": "reference",
                                         "sample": f"unavailable: {e}"}
         print(json.dumps(line), flush=True)
+    net.close()
 
 
 BATCH_MODELS = ("vogels_abbott", "brunel", "brunel_with_plasticity")

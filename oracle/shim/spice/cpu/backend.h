@@ -21,8 +21,10 @@
 
 namespace oracle
 {
-// One net per process at a time: the harness sets these before constructing a net.
-struct counter_rng
+// One net per library at a time: the harness sets these before constructing a net. Hidden,
+// so that the two builds (parity and fast) loaded into one process keep separate counters
+// (default-visibility inline variables would be merged across the libraries).
+struct __attribute__( ( visibility( "hidden" ) ) ) counter_rng
 {
 	static inline uint64_t seed = 1;
 	static inline uint64_t npoisson = 1;

@@ -202,3 +202,38 @@ def test_oracle_matches_reference_live():
             assert np.array_equal(r.step(), o.step()), (model, i)
         for x, y in zip(r.neurons(), o.neurons()):
             assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+@pytest.mark.parametrize("model,pops,conns,delay", [
+    ("brunel", [1500, 1500], [(0, 1, 0.1), (1, 1, 0.1)], 15),
+    ("vogels_abbott", [2000], [(0, 0, 0.02)], 1),
+    ("brunel_with_plasticity", [300, 300], [(0, 1, 0.1), (1, 1, 0.1)], 15),
+])
+def test_continuation_from_exported_state(model, pops, conns, delay):
+    """A net handed the graph, state, clock and spikes in flight of another net at step S
+    continues exactly as the original does: the restatement (set_state / set_progress) and
+    the reference's cpu::snn (ReferenceNet.from_state), against an uninterrupted run. The
+    GPU parity tests at full size and the benchmark's CPU leg rest on this."""
+    o = oracle.OracleNet(model, pops, conns, delay=delay, seed=3, graph="philox", graph_seed=3)
+    S = 900
+    for _ in range(S - delay):
+        o.step()
+    rec = [o.step() for _ in range(delay)]
+    counts, ids = [len(r) for r in rec], np.concatenate(rec)
+    e, w = o.adj()
+    st, sy = o.neurons(), o.synapses() or None
+    c = oracle.OracleNet(model, pops, conns, delay=delay, seed=3, edges=e, width=w)
+    c.set_state(st, sy)
+    c.set_progress(S, counts, ids)
+    nets = [c]
+    if oracle.have_reference():
+        nets.append(oracle.ReferenceNet.from_state(model, e, w, st, sy, delay=delay, seed=3, step0=S, counts=counts, ids=ids))
+    for i in range(1200):
+        want = o.step()
+        for x in nets:
+            assert np.array_equal(x.step(), want), i
+    for x in nets:
+        for a, b in zip(x.neurons(), o.neurons()):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        for a, b in zip(x.synapses(), o.synapses()):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
