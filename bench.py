@@ -32,6 +32,16 @@ SIM_STEPS = 1050                      # per bench step
 METRIC = "wall/bio time ratio at 1e9-syn Brunel"
 
 
+# single-net workloads: model, populations, connections, delay, synapses
+MODEL_WORKLOADS = {
+    "va": ("vogels_abbott", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02),
+    "va_ns": ("vogels_abbott_ns", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02),
+    "brunel_plus": ("brunel_with_plasticity", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8),
+    "brunel_plus_a012": ("brunel_with_plasticity_a012", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8),
+    "brunel_fixed": ("brunel_fixed", [70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1e9),
+}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -42,10 +52,11 @@ def parse():
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--syn", type=float, default=1e9,
                     help="total synapses of the Brunel net (the benchmark is 1e9; smaller sizes serve profiling)")
-    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched", "serving", "va", "brunel_plus"],
+    ap.add_argument("--workload", default="brunel", choices=["brunel", "batched", "serving"] + list(MODEL_WORKLOADS),
                     help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop; "
                          "serving: Poisson job arrivals, server vs plain per-job loop; va: Vogels-Abbott 4000+1000 "
-                         "at delay 1; brunel_plus: Brunel with STDP at 5e8 synapses")
+                         "at delay 1; brunel_plus: Brunel with STDP at 5e8 synapses; va_ns, brunel_fixed, "
+                         "brunel_plus_a012: the same with the benchmark configurations' model constants")
     ap.add_argument("--duration", type=float, default=8.0, help="serving: seconds of job arrivals")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: job arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
@@ -602,10 +613,7 @@ def run_model_workload(args, rank, world):
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    if args.workload == "va":
-        model, pops, conns, delay, syn = "vogels_abbott", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02
-    else:
-        model, pops, conns, delay, syn = "brunel_with_plasticity", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8
+    model, pops, conns, delay, syn = MODEL_WORKLOADS[args.workload]
     steps = int(round(args.bio / DT))
     t0 = time.perf_counter()
     net = Snn(model, Layout(pops, conns), dt=DT, delay=delay, seed=1 + rank, graph_seed=1337 + rank, device=dev)
@@ -639,12 +647,22 @@ def run_model_workload(args, rank, world):
             "e2e": {"value": e2e / (steps * DT), "unit": "wall_s/bio_s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int((counts.nbytes + ids.nbytes) / 1)},
             "gpu_launches": info.kernel_launches, "clocks": clk}
+    rates = {}
+    if counts.sum():
+        n = sum(pops)
+        groups = {"exc": (0, int(0.8 * n)), "inh": (int(0.8 * n), n)} if model.startswith("vogels") else \
+                 {"poisson": (0, n // 2), "exc": (n // 2, int(0.9 * n)), "inh": (int(0.9 * n), n)}
+        hist = np.bincount(ids, minlength=n)
+        rates = {k: float(hist[a:b].sum()) / (b - a) / (steps * DT) for k, (a, b) in groups.items()}
+    line["rates_hz"] = rates
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
 
-        fast = oracle.have_reference(fast=True)
-        cpu_pops = pops if args.workload == "va" else [2000, 2000]
-        cpu_steps = steps if args.workload == "va" else 200
+        small = syn > 1e7  # the CPU runs the full net only where it finishes in seconds
+        reference_model = model in oracle.REFERENCE_MODELS
+        fast = oracle.have_reference(fast=True) and reference_model
+        cpu_pops = [2000, 2000] if small else pops
+        cpu_steps = 200 if small else steps
         mk = (lambda: oracle.ReferenceNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, fast=True)) if fast else \
              (lambda: oracle.OracleNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, graph="reference", graph_seed=1337))
         cpu = mk()
@@ -655,7 +673,8 @@ def run_model_workload(args, rank, world):
         line["cpu_baseline"] = {"value": wall / (cpu_steps * DT), "unit": "wall_s/bio_s", "cores": 1,
                                 "kind": "reference" if fast else "port",
                                 "sample": f"{model} N={sum(cpu_pops)}, {cpu_steps} steps, single thread"
-                                          + ("" if args.workload == "va" else " (small N: the CPU STDP sweep is eager over all synapses)")}
+                                          + (" (small N: the full net takes minutes per step on one core)" if small else "")
+                                          + ("" if reference_model else " (the reference has no such model: the port runs it)")}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -670,7 +689,7 @@ def main():
             run_batched(args, rank, world)
         elif args.workload == "serving":
             run_serving(args, rank, world)
-        elif args.workload in ("va", "brunel_plus"):
+        elif args.workload in MODEL_WORKLOADS:
             run_model_workload(args, rank, world)
         else:
             run_ours(args, rank, world)

@@ -6,9 +6,12 @@
 #pragma once
 
 #include <spice/models/brunel.h>
+#include <spice/models/brunel_fixed.h>
 #include <spice/models/brunel_with_plasticity.h>
+#include <spice/models/brunel_with_plasticity_a012.h>
 #include <spice/models/synth.h>
 #include <spice/models/vogels_abbott.h>
+#include <spice/models/vogels_abbott_ns.h>
 #include <spice/snn.h>
 #include <spice/util/layout.h>
 #include <spice_b200.h>
@@ -44,6 +47,18 @@ struct model_id<brunel_with_plasticity> : std::integral_constant<int, SPK_BRUNEL
 };
 template <>
 struct model_id<synth> : std::integral_constant<int, SPK_SYNTH>
+{
+};
+template <>
+struct model_id<vogels_abbott_ns> : std::integral_constant<int, SPK_VOGELS_ABBOTT_NS>
+{
+};
+template <>
+struct model_id<brunel_fixed> : std::integral_constant<int, SPK_BRUNEL_FIXED>
+{
+};
+template <>
+struct model_id<brunel_with_plasticity_a012> : std::integral_constant<int, SPK_BRUNEL_PLUS_A012>
 {
 };
 

@@ -33,7 +33,12 @@ typedef enum spk_model
 	SPK_VOGELS_ABBOTT = 0, /* spice/models/vogels_abbott.h          */
 	SPK_BRUNEL = 1,        /* spice/models/brunel.h                 */
 	SPK_BRUNEL_PLUS = 2,   /* spice/models/brunel_with_plasticity.h */
-	SPK_SYNTH = 3          /* spice/models/synth.h                  */
+	SPK_SYNTH = 3,         /* spice/models/synth.h                  */
+	/* the same models with the benchmark configurations' constants (no reference
+	   counterpart; see each header): */
+	SPK_VOGELS_ABBOTT_NS = 4, /* include/spice/models/vogels_abbott_ns.h: 0.27 / 4.5 nS, V uniform in [-60, -50) mV */
+	SPK_BRUNEL_FIXED = 5,     /* include/spice/models/brunel_fixed.h: reset 10 mV, J = 0.1 / -0.5 mV */
+	SPK_BRUNEL_PLUS_A012 = 6  /* include/spice/models/brunel_with_plasticity_a012.h: A- = 0.012 */
 } spk_model;
 
 /* Population sizes and (src_pop, dst_pop, p) connection list: the arguments of
@@ -324,6 +329,11 @@ int spk_server_get_stats( spk_server * server, spk_server_stats * out );
 /* Fault injection on the host: the next `count` admissions fail as an allocation failure
  * would (the job ends FAILED with SPK_ERR_NOMEM; the server carries on). */
 int spk_server_inject_alloc_failures( spk_server * server, int count );
+/* Fault injection on the host: at the job's next tick its net reports a device error, as
+ * when a kernel's bounded wait runs out (its error word set); the job ends FAILED with
+ * SPK_ERR_DEVICE and the other jobs carry on. SPK_ERR_INVALID for an unknown or finished
+ * job. */
+int spk_server_inject_device_error( spk_server * server, uint64_t job );
 /* Stops both threads; queued and running jobs are dropped. */
 int spk_server_destroy( spk_server * server );
 

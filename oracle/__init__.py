@@ -22,8 +22,12 @@ REF_FAST_LIB = os.path.join(HERE, "_ref", "libspice_ref_fast.so")
 # the reference checkout the `ref` build compiles from (no default: set by the build recipe)
 REFERENCE_SRC = os.environ.get("SPICE_REFERENCE_SRC", "")
 
-MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3}
-NEURON_ATTRS = {0: [np.float32] * 3 + [np.int32], 1: [np.float32, np.int32], 2: [np.float32, np.int32], 3: [np.int32]}
+MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3,
+          "vogels_abbott_ns": 4, "brunel_fixed": 5, "brunel_with_plasticity_a012": 6}
+NEURON_ATTRS = {0: [np.float32] * 3 + [np.int32], 1: [np.float32, np.int32], 2: [np.float32, np.int32], 3: [np.int32],
+                4: [np.float32] * 3 + [np.int32], 5: [np.float32, np.int32], 6: [np.float32, np.int32]}
+PLASTIC = (2, 6)
+REFERENCE_MODELS = ("vogels_abbott", "brunel", "brunel_with_plasticity", "synth")  # the reference's own structs
 
 U64P, IP, FP = C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_float)
 
@@ -190,7 +194,7 @@ class OracleNet:
             raise ValueError(oracle_lib().oracle_last_error().decode())
 
     def synapses(self):
-        if self.model != 2:
+        if self.model not in PLASTIC:
             return []
         dt = np.float32 if self.precision == 32 else np.float64
         arrs = [np.empty(self.n * self.width, dtype=dt) for _ in range(3)]
@@ -289,7 +293,7 @@ class ReferenceNet:
         return arrs
 
     def synapses(self):
-        if self.model != 2:
+        if self.model not in PLASTIC:
             return []
         arrs = [np.empty(self.n * self.width, dtype=np.float32) for _ in range(3)]
         self.lib.ref_synapses(self._h, (C.c_void_p * 3)(*[a.ctypes.data for a in arrs]))

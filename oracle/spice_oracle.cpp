@@ -282,8 +282,21 @@ enum model_id
 	VOGELS_ABBOTT = 0,
 	BRUNEL = 1,
 	BRUNEL_PLUS = 2,
-	SYNTH = 3
+	SYNTH = 3,
+	// the benchmark configurations' constants (include/spice/models/vogels_abbott_ns.h,
+	// brunel_fixed.h, brunel_with_plasticity_a012.h): the model above them, with the
+	// differences restated where they apply
+	VOGELS_ABBOTT_NS = 4,
+	BRUNEL_FIXED = 5,
+	BRUNEL_PLUS_A012 = 6
 };
+constexpr int MODEL_COUNT = 7;
+
+// the reference model a variant differs from
+static int base_model( int m )
+{
+	return m == VOGELS_ABBOTT_NS ? VOGELS_ABBOTT : m == BRUNEL_FIXED ? BRUNEL : m == BRUNEL_PLUS_A012 ? BRUNEL_PLUS : m;
+}
 
 template <typename R>
 struct state
@@ -321,10 +334,14 @@ struct sim
 	void init_state()
 	{
 		int const n = s.n;
-		switch( s.model )
+		switch( base_model( s.model ) )
 		{
 		case VOGELS_ABBOTT: // vogels_abbott.h:23-33
 			s.V.assign( n, K<R>( -0.06 ) );
+			if( s.model == VOGELS_ABBOTT_NS ) // uniform in [-60, -50) mV from the initialisation draw
+				for( int i = 0; i < n; i++ )
+					s.V[i] = K<R>( -0.06 ) + ( K<R>( -0.05 ) - K<R>( -0.06 ) ) *
+					                             static_cast<R>( uniform_left_inc( neuron_u32( rng_seed, (uint32_t)i, 0xFFFFFFFFu, 0 ) ) );
 			s.Gex.assign( n, R( 0 ) );
 			s.Gin.assign( n, R( 0 ) );
 			s.Twait.assign( n, 0 );
@@ -338,7 +355,7 @@ struct sim
 			s.Ncount.assign( n, 0 );
 			break;
 		}
-		if( s.model == BRUNEL_PLUS ) // brunel_with_plasticity.h:83-100
+		if( base_model( s.model ) == BRUNEL_PLUS ) // brunel_with_plasticity.h:83-100
 		{
 			s.W.assign( edges.size(), R( 0 ) );
 			s.Zpre.assign( edges.size(), R( 0 ) );
@@ -360,7 +377,7 @@ struct sim
 	bool update( int i, R dt_ )
 	{
 		int const n = s.n;
-		switch( s.model )
+		switch( base_model( s.model ) )
 		{
 		case VOGELS_ABBOTT:
 		{ // vogels_abbott.h:35-71
@@ -404,7 +421,8 @@ struct sim
 			{
 				if( V > Vthres )
 				{
-					V = Vrest;
+					// brunel_fixed resets to 10 mV
+					V = s.model == BRUNEL_FIXED ? K<R>( 0.01 ) : Vrest;
 					Tw = Tref;
 					return true;
 				}
@@ -422,12 +440,13 @@ struct sim
 	void receive( int src, int dst, size_t syn )
 	{
 		int const n = s.n;
-		switch( s.model )
+		switch( base_model( s.model ) )
 		{
 		case VOGELS_ABBOTT:
-		{ // vogels_abbott.h:73-89
-			R const Wex = K<R>( 0.4 ) * R( 16000000 ) / static_cast<R>( (int64_t)n * n );
-			R const Win = K<R>( 5.1 ) * R( 16000000 ) / static_cast<R>( (int64_t)n * n );
+		{ // vogels_abbott.h:73-89; vogels_abbott_ns: 0.27 nS and 4.5 nS over the 10 nS leak
+			bool const ns = s.model == VOGELS_ABBOTT_NS;
+			R const Wex = ns ? K<R>( 0.27 ) / K<R>( 10 ) : K<R>( 0.4 ) * R( 16000000 ) / static_cast<R>( (int64_t)n * n );
+			R const Win = ns ? K<R>( 4.5 ) / K<R>( 10 ) : K<R>( 5.1 ) * R( 16000000 ) / static_cast<R>( (int64_t)n * n );
 			int const nexc = static_cast<int>( K<R>( 0.8 ) * n );
 			if( src < nexc )
 				s.Gex[dst] += Wex;
@@ -440,8 +459,10 @@ struct sim
 			if( s.Twait[dst] <= 0 )
 			{
 				int const nexc = static_cast<int>( K<R>( 0.9 ) * n );
-				R const Wex = K<R>( 0.0001 ) * R( 20000 ) / static_cast<R>( n );
-				R const Win = K<R>( -0.0005 ) * R( 20000 ) / static_cast<R>( n );
+				// brunel_fixed: J = 0.1 / -0.5 mV, not scaled by 20,000 / N
+				bool const fixed = s.model == BRUNEL_FIXED;
+				R const Wex = fixed ? K<R>( 0.0001 ) : K<R>( 0.0001 ) * R( 20000 ) / static_cast<R>( n );
+				R const Win = fixed ? K<R>( -0.0005 ) : K<R>( -0.0005 ) * R( 20000 ) / static_cast<R>( n );
 				s.V[dst] += src < nexc ? Wex : Win;
 			}
 			break;
@@ -466,7 +487,8 @@ struct sim
 		R & w = s.W[syn];
 		zpre = std::fma( zpre, decay, static_cast<R>( pre ) );
 		zpost = std::fma( zpost, decay, static_cast<R>( post ) );
-		R const x = w - pre * K<R>( 0.0202 ) * w * std::exp( -zpost * dtInv ) +
+		R const a_minus = s.model == BRUNEL_PLUS_A012 ? K<R>( 0.012 ) : K<R>( 0.0202 );
+		R const x = w - pre * a_minus * w * std::exp( -zpost * dtInv ) +
 		            post * K<R>( 0.01 ) * ( R( 1 ) - w ) * std::exp( -zpre * dtInv );
 		w = std::min( K<R>( 0.0003 ), std::max( R( 0 ), x ) );
 	}
@@ -499,12 +521,12 @@ struct sim
 		for( int i = 0; i < n; i++ )
 		{
 			bool const spiked = update( i, dt_ );
-			if( s.model == BRUNEL_PLUS ) flags[post][i] = spiked;
+			if( base_model( s.model ) == BRUNEL_PLUS ) flags[post][i] = spiked;
 			if( spiked ) out.push_back( i );
 		}
 		queue.push_back( out );
 
-		if( s.model == BRUNEL_PLUS )
+		if( base_model( s.model ) == BRUNEL_PLUS )
 		{
 			// every synapse's update reads only its own state and the step's flags, so rows
 			// are independent: large nets sweep them on several threads (same results)
@@ -572,7 +594,7 @@ static void export_neurons( sim<R> & s, double ** a )
 	auto put = [&]( double * dst, auto const & v ) {
 		for( size_t i = 0; i < v.size(); i++ ) dst[i] = (double)v[i];
 	};
-	switch( s.s.model )
+	switch( base_model( s.s.model ) )
 	{
 	case VOGELS_ABBOTT:
 		put( a[0], s.s.V ), put( a[1], s.s.Gex ), put( a[2], s.s.Gin ), put( a[3], s.s.Twait );
@@ -689,7 +711,7 @@ void * oracle_create(
 	{
 		if( !( dt > 0.0f ) ) throw std::invalid_argument( "dt must be > 0" );
 		if( delay < 1 ) throw std::invalid_argument( "delay must be >= 1" );
-		if( model < 0 || model > 3 ) throw std::invalid_argument( "invalid model" );
+		if( model < 0 || model >= MODEL_COUNT ) throw std::invalid_argument( "invalid model" );
 		auto build = [&]( auto * h ) -> void * {
 			auto & s = h->s;
 			s.lay = layout_from( npops, pops, nconn, csrc, cdst, cp );
@@ -790,14 +812,14 @@ void oracle_set_state( void * h, void * const * neurons, void * const * synapses
 			for( size_t i = 0; i < dst.size(); i++ ) dst[i] = static_cast<R>( f[i] );
 		};
 		auto in = [&]( std::vector<int> & dst, void const * src ) { std::memcpy( dst.data(), src, dst.size() * 4 ); };
-		switch( s.s.model )
+		switch( base_model( s.s.model ) )
 		{
 		case VOGELS_ABBOTT: fl( s.s.V, neurons[0] ), fl( s.s.Gex, neurons[1] ), fl( s.s.Gin, neurons[2] ), in( s.s.Twait, neurons[3] ); break;
 		case BRUNEL:
 		case BRUNEL_PLUS: fl( s.s.V, neurons[0] ), in( s.s.Twait, neurons[1] ); break;
 		case SYNTH: in( s.s.Ncount, neurons[0] ); break;
 		}
-		if( s.s.model == BRUNEL_PLUS && synapses ) fl( s.s.W, synapses[0] ), fl( s.s.Zpre, synapses[1] ), fl( s.s.Zpost, synapses[2] );
+		if( base_model( s.s.model ) == BRUNEL_PLUS && synapses ) fl( s.s.W, synapses[0] ), fl( s.s.Zpre, synapses[1] ), fl( s.s.Zpost, synapses[2] );
 	};
 	if( is64( h ) )
 		go( S<double>( h ) );
@@ -820,7 +842,7 @@ int oracle_set_progress( void * h, uint64_t step0, int nq, uint32_t const * coun
 		for( int q = 0; q < nq; q++ )
 		{
 			s.queue.emplace_back( ids + o, ids + o + counts[q] );
-			if( s.s.model == BRUNEL_PLUS )
+			if( base_model( s.s.model ) == BRUNEL_PLUS )
 				for( uint32_t k = 0; k < counts[q]; k++ ) s.flags[( step0 - nq + q ) % ( s.delay + 1 )][ids[o + k]] = 1;
 			o += counts[q];
 		}
@@ -845,7 +867,7 @@ void oracle_neurons_f32( void * h, void ** a )
 {
 	auto & s = S<float>( h );
 	auto cpy = [&]( void * dst, auto const & v ) { std::memcpy( dst, v.data(), v.size() * 4 ); };
-	switch( s.s.model )
+	switch( base_model( s.s.model ) )
 	{
 	case VOGELS_ABBOTT: cpy( a[0], s.s.V ), cpy( a[1], s.s.Gex ), cpy( a[2], s.s.Gin ), cpy( a[3], s.s.Twait ); break;
 	case BRUNEL:

@@ -21,7 +21,9 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libspice_b200.so")
 
-MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3}
+MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3,
+          # the benchmark configurations' constants (include/spice/models/*.h)
+          "vogels_abbott_ns": 4, "brunel_fixed": 5, "brunel_with_plasticity_a012": 6}
 MODEL_NAMES = {v: k for k, v in MODELS.items()}
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_DEVICE, ERR_CAPACITY, ERR_TIMEOUT = range(7)
@@ -141,6 +143,7 @@ def library():
         "spk_server_wait": (I, [VP, U64, C.c_double]),
         "spk_server_get_stats": (I, [VP, P(ServerStats)]),
         "spk_server_inject_alloc_failures": (I, [VP, I]),
+        "spk_server_inject_device_error": (I, [VP, U64]),
         "spk_server_destroy": (I, [VP]),
         "spk_batch_create": (I, [P(VP), I]),
         "spk_batch_add": (I, [VP, VP]),
@@ -230,11 +233,12 @@ class Snn:
     """One simulated network on one GPU: the reference's cuda::snn<Model>.
 
     Snn(model, layout, dt, delay=1, seed=1, graph_seed=1337)   generate the graph on device
+                                                                (tile_target: tiles for a GPU shared with others)
     Snn(model, adj=(edges, width), dt=..., delay=...)           import an ELL adjacency
     Snn.from_state(model, edges, width, neurons, synapses, ...)  conversion constructor
     """
 
-    def __init__(self, model, layout=None, dt=1e-4, delay=1, seed=1, graph_seed=1337, device=0, adj=None):
+    def __init__(self, model, layout=None, dt=1e-4, delay=1, seed=1, graph_seed=1337, device=0, adj=None, tile_target=0):
         lib = library()
         self.model = model if isinstance(model, str) else MODEL_NAMES[int(model)]
         m = MODELS[self.model]
@@ -250,8 +254,8 @@ class Snn:
             if layout is None:
                 raise InvalidArgument(ERR_INVALID, "layout or adj required")
             d = layout.desc()
-            _check(lib.spk_net_create(C.byref(self._h), m, C.byref(d), float(dt), int(delay), int(seed), int(graph_seed),
-                                      int(device)))
+            _check(lib.spk_net_create_ex(C.byref(self._h), m, C.byref(d), float(dt), int(delay), int(seed), int(graph_seed),
+                                         int(device), int(tile_target)))
         self._ndt, self._sdt = model_attrs(self.model)
 
     @classmethod
@@ -509,6 +513,11 @@ class Server:
 
     def inject_alloc_failures(self, count):
         _check(library().spk_server_inject_alloc_failures(self._h, int(count)))
+
+    def inject_device_error(self, job):
+        """At its next tick the job's net reports a device error (as a bounded wait that ran
+        out does); the job fails alone."""
+        _check(library().spk_server_inject_device_error(self._h, int(job)))
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

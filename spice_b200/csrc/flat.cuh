@@ -534,7 +534,7 @@ __device__ __forceinline__ void compact_step( net_params const & p, unsigned con
 	// every lane's ring writes, then the flag that publishes them
 	__threadfence();
 	__syncwarp();
-	if( lane == 0 ) publish_step( p, tile, t );
+	if( lane == 0 && tile != p.withhold_tile ) publish_step( p, tile, t );
 }
 
 // neuron state of the tile: shared memory [attrs][span] <-> registers / global memory

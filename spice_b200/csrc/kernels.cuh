@@ -70,6 +70,8 @@ struct net_params
 	int pack;                // indices per 16-byte slice vector: 8 (16-bit) or 12 (10-bit)
 	int flat_sync;           // window_flat: every step on the synchronous path
 	long long * done_step;   // [ntiles] last step whose spikes the tile has published
+	int wait_limit;          // polls of a bounded wait before it gives up (WAIT_LIMIT)
+	int withhold_tile;       // failure-detection tests: this tile never publishes (-1: none)
 };
 
 template <typename T>
@@ -181,7 +183,7 @@ __device__ __forceinline__ void wait_published( net_params const & p, int i, lon
 	for( int it = 0; published( p, i ) < t; it++ )
 	{
 		// after one wait has given up, every other wait of the launch returns at once
-		if( it >= WAIT_LIMIT || ( *(int volatile *)p.err & ERR_TIMEOUT ) )
+		if( it >= p.wait_limit || ( *(int volatile *)p.err & ERR_TIMEOUT ) )
 		{
 			atomicOr( p.err, ERR_TIMEOUT );
 			return;

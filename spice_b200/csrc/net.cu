@@ -6,12 +6,9 @@
 // window); spk_net_run replays a captured CUDA graph of many windows.
 #include "kernels.cuh"
 #include "flat.cuh"
+#include "models.cuh"
 #include "plastic.cuh"
 
-#include <spice/models/brunel.h>
-#include <spice/models/brunel_with_plasticity.h>
-#include <spice/models/synth.h>
-#include <spice/models/vogels_abbott.h>
 #include <spice/util/layout.h>
 #include <spice_b200.h>
 
@@ -306,27 +303,24 @@ private:
 	}
 };
 
-struct model_desc
+spk::model_traits describe( int model )
 {
-	int neuron_attrs;
-	int synapse_attrs; // as exported (the reference's tuple)
-	char const * types;
-};
-
-model_desc describe( int model )
-{
-	switch( model )
-	{
-	case SPK_VOGELS_ABBOTT: return { 4, 0, "fffi" };
-	case SPK_BRUNEL: return { 2, 0, "fi" };
-	case SPK_BRUNEL_PLUS: return { 2, 3, "fifff" };
-	case SPK_SYNTH: return { 1, 0, "i" };
-	default: throw spk_error( SPK_ERR_INVALID, "invalid model" );
-	}
+	spk::model_traits t{};
+	if( !spk::with_model( model, [&]( auto tag ) { t = spk::traits_of<typename decltype( tag )::type>(); } ) )
+		throw spk_error( SPK_ERR_INVALID, "invalid model" );
+	return t;
 }
 
-int classes_of( int model ) { return model == SPK_BRUNEL_PLUS ? 0 : ( model == SPK_SYNTH ? 1 : 2 ); }
-int neuron_attrs_of( int model ) { return model == SPK_VOGELS_ABBOTT ? 4 : ( model == SPK_SYNTH ? 1 : 2 ); }
+bool plastic_of( int model ) { return describe( model ).plastic; }
+int classes_of( int model ) { return describe( model ).classes; }
+int neuron_attrs_of( int model ) { return describe( model ).neuron_attrs; }
+
+// body( model_tag<Model> ) for the net's model (a valid id: checked at creation)
+template <typename F>
+void dispatch( int model, F && body )
+{
+	if( !spk::with_model( model, std::forward<F>( body ) ) ) throw spk_error( SPK_ERR_INVALID, "invalid model" );
+}
 
 spice::util::layout to_layout( spk_layout_desc const * d )
 {
@@ -419,7 +413,7 @@ struct spk_net
 	std::vector<int> tile_first_host; // [ntiles + 1]
 	dbuf attr[spk::MAX_ATTRS];
 	dbuf gather_ids, gather_cnt, cursor, gather_done, rec_ids, rec_cnt;
-	spk::plastic_state plast; // brunel_with_plasticity only
+	spk::plastic_state plast; // plastic models only
 
 	unsigned long long steps = 0;   // steps requested so far
 	unsigned long long launched = 0; // steps launched
@@ -440,6 +434,11 @@ struct spk_net
 	int pack = 8;           // slice indices per 16-byte vector: 8 (16-bit) or 12 (10-bit)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
 	bool persistent = false; // run() as one cooperative window_flat launch (delay >= 6)
+	// failure-detection tests (SPK_TEST_WAIT_LIMIT, SPK_TEST_WITHHOLD_TILE at creation): a
+	// shorter bounded wait, and a tile that never publishes its steps so that the waits of
+	// the tiles reading it run out and the launch ends with ERR_TIMEOUT in the error word
+	int wait_limit = spk::WAIT_LIMIT;
+	int withhold_tile = -1;
 	std::vector<double> seg_start, seg_cost; // expected work per neuron stretch (tiling)
 	spk_batch * batch = nullptr;             // the batch holding this net, if any
 
@@ -476,6 +475,8 @@ struct spk_net
 		p.flat_sync = flat_sync;
 		p.pack = pack;
 		p.done_step = done_step.as<long long>();
+		p.wait_limit = wait_limit;
+		p.withhold_tile = withhold_tile;
 		return p;
 	}
 
@@ -497,7 +498,7 @@ struct spk_net
 		int const classes = this->classes();
 		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
 		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
-		if( model == SPK_BRUNEL_PLUS ) b = spk::plastic_window_smem( tc.tile, tc.ntiles, tc.threads );
+		if( plastic_of( model ) ) b = spk::plastic_window_smem( tc.tile, tc.ntiles, tc.threads );
 		return (int)b;
 	}
 
@@ -571,13 +572,7 @@ struct spk_net
 
 	void configure()
 	{
-		switch( model )
-		{
-		case SPK_VOGELS_ABBOTT: configure_model<spice::vogels_abbott>(); break;
-		case SPK_BRUNEL: configure_model<spice::brunel>(); break;
-		case SPK_BRUNEL_PLUS: configure_model<spice::brunel_with_plasticity>(); break;
-		case SPK_SYNTH: configure_model<spice::synth>(); break;
-		}
+		dispatch( model, [&]( auto tag ) { configure_model<typename decltype( tag )::type>(); } );
 	}
 
 	template <typename Model>
@@ -599,13 +594,7 @@ struct spk_net
 
 	void launch_window( int L )
 	{
-		switch( model )
-		{
-		case SPK_VOGELS_ABBOTT: launch_window_model<spice::vogels_abbott>( L ); break;
-		case SPK_BRUNEL: launch_window_model<spice::brunel>( L ); break;
-		case SPK_BRUNEL_PLUS: launch_window_model<spice::brunel_with_plasticity>( L ); break;
-		case SPK_SYNTH: launch_window_model<spice::synth>( L ); break;
-		}
+		dispatch( model, [&]( auto tag ) { launch_window_model<typename decltype( tag )::type>( L ); } );
 	}
 
 	int max_window() const { return std::min( delay, spk::MAX_WINDOW ); }
@@ -667,11 +656,12 @@ struct spk_net
 	void grow_ring( int slots )
 	{
 		if( slots <= ring_slots ) return;
-		require( flat && model != SPK_BRUNEL_PLUS && launched == steps, "ring growth of a window_flat net between runs" );
+		require( flat && !plastic_of( model ) && launched == steps, "ring growth of a window_flat net between runs" );
 		dbuf ids, cnt;
 		ids.alloc( (size_t)slots * n * 4, mem() );
 		cnt.alloc( (size_t)slots * tc.ntiles * 4, mem() );
 		CK( cudaMemsetAsync( cnt.p, 0, cnt.bytes, stream ) );
+		CK( cudaMemsetAsync( ids.p, 0, ids.bytes, stream ) );
 		long long const t = (long long)launched;
 		for( long long st = std::max( 0LL, t - ring_slots ); st < t; st++ )
 		{
@@ -723,13 +713,7 @@ struct spk_net
 	}
 	void launch_persistent( int L )
 	{
-		switch( model )
-		{
-		case SPK_VOGELS_ABBOTT: launch_persistent_model<spice::vogels_abbott>( L ); break;
-		case SPK_BRUNEL: launch_persistent_model<spice::brunel>( L ); break;
-		case SPK_SYNTH: launch_persistent_model<spice::synth>( L ); break;
-		default: break;
-		}
+		dispatch( model, [&]( auto tag ) { launch_persistent_model<typename decltype( tag )::type>( L ); } );
 	}
 
 	void run( unsigned long long nsteps )
@@ -782,13 +766,7 @@ void init_model( spk_net & net )
 
 void init_state( spk_net & net )
 {
-	switch( net.model )
-	{
-	case SPK_VOGELS_ABBOTT: init_model<spice::vogels_abbott>( net ); break;
-	case SPK_BRUNEL: init_model<spice::brunel>( net ); break;
-	case SPK_BRUNEL_PLUS: init_model<spice::brunel_with_plasticity>( net ); break;
-	case SPK_SYNTH: init_model<spice::synth>( net ); break;
-	}
+	dispatch( net.model, [&]( auto tag ) { init_model<typename decltype( tag )::type>( net ); } );
 }
 
 // Work per neuron, piecewise constant: neurons [start, next start) cost `cost` each.
@@ -1008,8 +986,8 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	int dev_sms = 0;
 	CK( cudaDeviceGetAttribute( &dev_sms, cudaDevAttrMultiProcessorCount, net.device ) );
 	net.sms = dev_sms;
-	net.tc = net.model == SPK_BRUNEL_PLUS ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
-	model_desc const md = describe( net.model );
+	net.tc = plastic_of( net.model ) ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
+	spk::model_traits const md = describe( net.model );
 
 	// window kernel and tiling: window_flat with work-balanced tiles (SPK_TILES=uniform keeps
 	// equal tiles, SPK_KERNEL=direct selects window_counts)
@@ -1022,7 +1000,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	}
 	net.flat = false;
 	char const * kern = getenv( "SPK_KERNEL" );
-	if( net.model != SPK_BRUNEL_PLUS && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, tile_target > 0 ? tile_target : dev_sms );
+	if( !plastic_of( net.model ) && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, tile_target > 0 ? tile_target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.ring_slots = 2 * net.delay;
 	allocate_buffers( net );
@@ -1033,7 +1011,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 void allocate_buffers( spk_net & net )
 {
 	long long const n = net.n, width = net.width;
-	model_desc const md = describe( net.model );
+	spk::model_traits const md = describe( net.model );
 	net.edges.alloc( (size_t)( n * width ) * 4, net.mem() );
 	net.pivots.alloc( (size_t)n * ( net.tc.ntiles + 1 ) * 4, net.mem() );
 	net.ring_ids.alloc( (size_t)net.ring_slots * n * 4, net.mem() );
@@ -1047,11 +1025,14 @@ void allocate_buffers( spk_net & net )
 	net.cursor.alloc( 8, net.mem() );
 	net.gather_done.alloc( 4, net.mem() );
 	CK( cudaMemsetAsync( net.ring_cnt.p, 0, net.ring_cnt.bytes, net.stream ) );
+	// spike ids start as valid neuron ids: a tile that reads a slot before its publication
+	// (only after a wait ran out) still indexes inside every table
+	CK( cudaMemsetAsync( net.ring_ids.p, 0, net.ring_ids.bytes, net.stream ) );
 	CK( cudaMemsetAsync( net.clock.p, 0, net.clock.bytes, net.stream ) );
 	CK( cudaMemsetAsync( net.err.p, 0, 4, net.stream ) );
 	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
 	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
-	if( net.model == SPK_BRUNEL_PLUS ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream, net.pool );
+	if( plastic_of( net.model ) ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream, net.pool );
 	if( !net.host_count ) net.host_count = pinned_slots::get();
 	net.configure();
 }
@@ -1101,13 +1082,7 @@ void build_slices( spk_net & net )
 	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
 	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ), net.mem() );
 	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)n * 8, cudaMemcpyHostToDevice, net.stream ) );
-	switch( net.model )
-	{
-	case SPK_VOGELS_ABBOTT: fill_slices<spice::vogels_abbott>( net, bases ); break;
-	case SPK_BRUNEL: fill_slices<spice::brunel>( net, bases ); break;
-	case SPK_SYNTH: fill_slices<spice::synth>( net, bases ); break;
-	default: break;
-	}
+	dispatch( net.model, [&]( auto tag ) { fill_slices<typename decltype( tag )::type>( net, bases ); } );
 	CK( cudaStreamSynchronize( net.stream ) ); // rows and bases are freed on return
 }
 
@@ -1202,7 +1177,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	bool flat = false;
 	long long T = 0;
 	int pack = 8;
-	if( model != SPK_BRUNEL_PLUS )
+	if( !plastic_of( model ) )
 	{
 		std::vector<int> first;
 		int span = 0;
@@ -1237,7 +1212,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 		b.push_back( (double)T * 8 );
 		b.push_back( (double)T * 4 );
 	}
-	if( model == SPK_BRUNEL_PLUS )
+	if( plastic_of( model ) )
 	{
 		b.push_back( (double)n * w * 4 );
 		for( int i = 0; i < 8; i++ ) b.push_back( (double)n * 4 );
@@ -1291,7 +1266,7 @@ std::vector<std::pair<uint32_t, void *>> ckpt_buffers( spk_net & net )
 std::vector<std::pair<uint32_t, spk::plastic_state::buf *>> ckpt_plastic( spk_net & net )
 {
 	auto & q = net.plast;
-	if( net.model != SPK_BRUNEL_PLUS ) return {};
+	if( !plastic_of( net.model ) ) return {};
 	return { { 40, &q.W },        { 41, &q.za },         { 42, &q.zpre },       { 43, &q.zpost },     { 44, &q.hist },
 	         { 45, &q.rf_a },     { 46, &q.zrf_a },      { 47, &q.rf_c },       { 48, &q.zrf_c },     { 49, &q.ring_meta },
 	         { 50, &q.flush_ring }, { 51, &q.flush_cnt }, { 52, &q.ring_pot } };
@@ -1324,7 +1299,7 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 {
 	uint64_t const n = (uint64_t)h.n, width = (uint64_t)h.width;
 	int const T = h.ntiles;
-	bool const plastic = h.model == SPK_BRUNEL_PLUS;
+	bool const plastic = plastic_of( h.model );
 	// the graph
 	int32_t const * edges = n * width ? reinterpret_cast<int32_t const *>( ckpt_find( dir, 1, n * width * 4 ) ) : nullptr;
 	if( edges )
@@ -1432,7 +1407,7 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	describe( model );
 	require( dt > 0.0f, "dt must be > 0" );
 	require( delay >= 1, "delay must be >= 1" );
-	require( model != SPK_BRUNEL_PLUS || delay <= spk::PL_MAX_DELAY, "plastic models support delays up to 63 steps" );
+	require( !plastic_of( model ) || delay <= spk::PL_MAX_DELAY, "plastic models support delays up to 63 steps" );
 	int ndev = 0;
 	CK( cudaGetDeviceCount( &ndev ) );
 	require( device >= 0 && device < ndev, "invalid device" );
@@ -1457,6 +1432,8 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	}
 	net->stream = net->owner.s;
 	if( pooled ) net->pool = scratch_pool( device );
+	if( char const * w = getenv( "SPK_TEST_WAIT_LIMIT" ) ) net->wait_limit = std::max( 1, atoi( w ) );
+	if( char const * h = getenv( "SPK_TEST_WITHHOLD_TILE" ) ) net->withhold_tile = atoi( h );
 	return net.release();
 }
 } // namespace
@@ -1486,7 +1463,7 @@ struct spk_batch
 	};
 	int device = 0;
 	std::vector<spk_net *> nets;
-	group groups[3]; // Vogels-Abbott, Brunel, synth
+	group groups[spk::MODEL_COUNT]; // by model id (models without plasticity only)
 
 	~spk_batch()
 	{
@@ -1500,8 +1477,7 @@ struct spk_batch
 	}
 
 	// stepped by the shared window_flat_batch launches
-	static bool shared( spk_net const & net ) { return net.flat && net.model != SPK_BRUNEL_PLUS; }
-	static int group_of( int model ) { return model == SPK_VOGELS_ABBOTT ? 0 : ( model == SPK_BRUNEL ? 1 : 2 ); }
+	static bool shared( spk_net const & net ) { return net.flat && !plastic_of( net.model ); }
 
 	template <typename Model>
 	static void launch_model( group & g, int4 const * jobs, int njobs, int smem )
@@ -1589,12 +1565,7 @@ struct spk_batch
 			for( auto const & l : launches )
 			{
 				int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
-				switch( model )
-				{
-				case SPK_VOGELS_ABBOTT: launch_model<spice::vogels_abbott>( g, jobs, l.second, smem ); break;
-				case SPK_BRUNEL: launch_model<spice::brunel>( g, jobs, l.second, smem ); break;
-				case SPK_SYNTH: launch_model<spice::synth>( g, jobs, l.second, smem ); break;
-				}
+				dispatch( model, [&]( auto tag ) { launch_model<typename decltype( tag )::type>( g, jobs, l.second, smem ); } );
 			}
 		};
 		// the rounds as one CUDA graph, captured once per job table and round sequence and
@@ -1632,22 +1603,21 @@ struct spk_batch
 	{
 		// nets outside window_flat (plastic ones) run their own windows on their own
 		// streams, concurrently with the shared launches
-		std::vector<spk_net *> gn[3];
-		std::vector<unsigned long long> gc[3];
+		std::vector<spk_net *> gn[spk::MODEL_COUNT];
+		std::vector<unsigned long long> gc[spk::MODEL_COUNT];
 		for( size_t i = 0; i < which.size(); i++ )
 		{
 			if( counts[i] == 0 ) continue;
 			if( shared( *which[i] ) )
 			{
-				gn[group_of( which[i]->model )].push_back( which[i] );
-				gc[group_of( which[i]->model )].push_back( counts[i] );
+				gn[which[i]->model].push_back( which[i] );
+				gc[which[i]->model].push_back( counts[i] );
 			}
 			else
 				which[i]->run( counts[i] );
 		}
-		int const models[3] = { SPK_VOGELS_ABBOTT, SPK_BRUNEL, SPK_SYNTH };
-		for( int m = 0; m < 3; m++ )
-			if( !gn[m].empty() ) run_group( groups[m], models[m], gn[m], gc[m] );
+		for( int m = 0; m < spk::MODEL_COUNT; m++ )
+			if( !gn[m].empty() ) run_group( groups[m], m, gn[m], gc[m] );
 	}
 };
 
@@ -1689,6 +1659,20 @@ void detach( spk_batch * b, spk_net * net )
 } // namespace
 
 void spk_set_last_error( std::string const & msg ) { g_err = msg; }
+
+// The serving loop's fault injection (spk_server_inject_device_error): the net's device
+// error word as a kernel sets it when a bounded wait runs out, so that its next
+// synchronisation reports SPK_ERR_DEVICE.
+int spk_net_raise_device_error( spk_net * net )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		device_guard g( net->device );
+		int const bits = spk::ERR_TIMEOUT;
+		CK( cudaMemcpyAsync( net->err.p, &bits, sizeof bits, cudaMemcpyHostToDevice, net->stream ) );
+		CK( cudaStreamSynchronize( net->stream ) );
+	} );
+}
 
 // A net whose buffers come from the device's stream-ordered pool (on the net's stream):
 // neither building nor destroying it synchronises the device, so the server's builder
@@ -1827,7 +1811,7 @@ int spk_net_set_neurons( spk_net * net, void * const * attrs )
 		require( net && attrs, "null argument" );
 		device_guard g( net->device );
 		net->flush();
-		model_desc const md = describe( net->model );
+		spk::model_traits const md = describe( net->model );
 		for( int i = 0; i < md.neuron_attrs; i++ )
 			CK( cudaMemcpyAsync( net->attr[i].p, attrs[i], (size_t)net->n * 4, cudaMemcpyHostToDevice, net->stream ) );
 		CK( cudaStreamSynchronize( net->stream ) );
@@ -1840,12 +1824,15 @@ int spk_net_set_synapses( spk_net * net, void * const * attrs )
 		require( net && attrs, "null argument" );
 		device_guard g( net->device );
 		net->flush();
-		model_desc const md = describe( net->model );
+		spk::model_traits const md = describe( net->model );
 		if( md.synapse_attrs == 0 ) return;
 		require( net->steps == 0, "synapse state can only be imported before the first step" );
-		net->plast.import<spice::brunel_with_plasticity>( net->params(), static_cast<float const *>( attrs[0] ),
-		                                                  static_cast<float const *>( attrs[1] ), static_cast<float const *>( attrs[2] ),
-		                                                  net->dt, net->sms, net->stream );
+		dispatch( net->model, [&]( auto tag ) {
+			using M = typename decltype( tag )::type;
+			if constexpr( spk::is_plastic_model<M> )
+				net->plast.import<M>( net->params(), static_cast<float const *>( attrs[0] ), static_cast<float const *>( attrs[1] ),
+				                      static_cast<float const *>( attrs[2] ), net->dt, net->sms, net->stream );
+		} );
 		CK( cudaStreamSynchronize( net->stream ) );
 	} );
 }
@@ -2025,7 +2012,7 @@ int spk_net_neurons( spk_net * net, void * const * attrs )
 		require( net && attrs, "null argument" );
 		device_guard g( net->device );
 		net->sync();
-		model_desc const md = describe( net->model );
+		spk::model_traits const md = describe( net->model );
 		for( int i = 0; i < md.neuron_attrs; i++ )
 			CK( cudaMemcpyAsync( attrs[i], net->attr[i].p, (size_t)net->n * 4, cudaMemcpyDeviceToHost, net->stream ) );
 		CK( cudaStreamSynchronize( net->stream ) );
@@ -2038,11 +2025,14 @@ int spk_net_synapses( spk_net * net, void * const * attrs )
 		require( net && attrs, "null argument" );
 		device_guard g( net->device );
 		net->sync();
-		model_desc const md = describe( net->model );
+		spk::model_traits const md = describe( net->model );
 		if( md.synapse_attrs == 0 ) return;
-		CK( net->plast.export_synapses<spice::brunel_with_plasticity>(
-		    net->params(), static_cast<float *>( attrs[0] ), static_cast<float *>( attrs[1] ), static_cast<float *>( attrs[2] ), net->sms,
-		    net->stream ) );
+		dispatch( net->model, [&]( auto tag ) {
+			using M = typename decltype( tag )::type;
+			if constexpr( spk::is_plastic_model<M> )
+				CK( net->plast.export_synapses<M>( net->params(), static_cast<float *>( attrs[0] ), static_cast<float *>( attrs[1] ),
+				                                   static_cast<float *>( attrs[2] ), net->sms, net->stream ) );
+		} );
 		CK( cudaStreamSynchronize( net->stream ) );
 	} );
 }
@@ -2181,7 +2171,7 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 int spk_model_attrs( int model, int * num_neuron_attrs, int * num_synapse_attrs, char * types, int types_cap )
 {
 	return guarded( [&] {
-		model_desc const md = describe( model );
+		spk::model_traits const md = describe( model );
 		if( num_neuron_attrs ) *num_neuron_attrs = md.neuron_attrs;
 		if( num_synapse_attrs ) *num_synapse_attrs = md.synapse_attrs;
 		if( types && types_cap > 0 )

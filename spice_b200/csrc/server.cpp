@@ -39,6 +39,17 @@ int spk_net_create_pooled(
     spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target );
 void spk_trim_pool( int device );
 void spk_reserve_pool( int device, uint64_t bytes );
+int spk_net_raise_device_error( spk_net * net );
+
+namespace
+{
+// models with plastic synapses export synapse attributes (spk_model_attrs)
+bool plastic_model( int model )
+{
+	int na = 0, ns = 0;
+	return spk_model_attrs( model, &na, &ns, nullptr, 0 ) == SPK_OK && ns > 0;
+}
+} // namespace
 
 namespace
 {
@@ -77,6 +88,7 @@ struct job
 	uint64_t num_neurons = 0;
 	double t_submit = 0, t_start = -1, t_end = -1;
 	bool cancel = false;
+	bool raise = false; // fault injection: its net reports a device error at its next tick
 	spk_net * net = nullptr;
 	double work = 0;                           // expected cost per step (tiling share)
 	bool own = false;                          // steps on its own stream, not in the shared launches (Brunel+)
@@ -196,6 +208,15 @@ struct server
 				finish( j, SPK_JOB_FAILED, rc, msg );
 				continue;
 			}
+			// held against the budget: the estimate, or what the net holds if that is more
+			// (admission stays within the budget even where an estimate falls short)
+			spk_net_info info{};
+			if( spk_net_get_info( j.net, &info ) == SPK_OK && info.device_bytes > j.reserved )
+			{
+				in_use += info.device_bytes - j.reserved;
+				j.reserved = info.device_bytes;
+				peak = std::max( peak, in_use );
+			}
 			ready.push_back( &j );
 			tick_wake.notify_all();
 		}
@@ -219,7 +240,7 @@ struct server
 				{
 					// nets outside the shared launches run on their own streams, each at its
 					// own pace: the ticks of the shared launches do not wait for them
-					j->own = info.model == SPK_BRUNEL_PLUS || info.slice_pack == 0;
+					j->own = plastic_model( info.model ) || info.slice_pack == 0;
 					running_t.push_back( j );
 				}
 				else
@@ -247,9 +268,14 @@ struct server
 			// own-stream jobs: a finished quantum is counted and the next one launched
 			std::vector<spk_net *> nets;
 			std::vector<uint64_t> counts;
-			std::vector<job *> ticked, owns;
+			std::vector<job *> ticked, owns, raised;
 			for( auto * j : running_t )
 			{
+				if( j->raise )
+				{
+					raised.push_back( j );
+					j->raise = false;
+				}
 				if( j->own )
 					owns.push_back( j );
 				else if( !j->cancel && j->done < j->nsteps )
@@ -260,6 +286,7 @@ struct server
 				}
 			}
 			lk.unlock();
+			for( auto * j : raised ) spk_net_raise_device_error( j->net );
 			double const tt = now();
 			std::vector<int> status( ticked.size(), SPK_OK );
 			std::vector<std::string> msgs( ticked.size() );
@@ -438,7 +465,7 @@ int spk_server_submit(
 {
 	if( !s || !desc || !out_job ) return fail( SPK_ERR_INVALID, "null argument" );
 	if( nsteps == 0 ) return fail( SPK_ERR_INVALID, "nsteps must be > 0" );
-	if( model == SPK_BRUNEL_PLUS && delay > 63 ) return fail( SPK_ERR_INVALID, "plastic models support delays up to 63 steps" );
+	if( plastic_model( model ) && delay > 63 ) return fail( SPK_ERR_INVALID, "plastic models support delays up to 63 steps" );
 	if( desc->npops <= 0 || !desc->pops || desc->nconn < 0 || ( desc->nconn && ( !desc->conn_src || !desc->conn_dst || !desc->conn_p ) ) )
 		return fail( SPK_ERR_INVALID, "bad layout descriptor" );
 	auto j = std::make_unique<job>();
@@ -595,6 +622,16 @@ int spk_server_inject_alloc_failures( spk_server * s, int count )
 	if( !s || count < 0 ) return fail( SPK_ERR_INVALID, "bad argument" );
 	std::lock_guard<std::mutex> lk( s->mu );
 	s->inject = count;
+	return SPK_OK;
+}
+
+int spk_server_inject_device_error( spk_server * s, uint64_t id )
+{
+	if( !s ) return fail( SPK_ERR_INVALID, "bad argument" );
+	std::lock_guard<std::mutex> lk( s->mu );
+	auto it = s->jobs.find( id );
+	if( it == s->jobs.end() || it->second->final() ) return fail( SPK_ERR_INVALID, "no such unfinished job" );
+	it->second->raise = true;
 	return SPK_OK;
 }
 

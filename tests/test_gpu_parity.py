@@ -91,7 +91,8 @@ def test_generator_large_rows_sampled():
 
 
 # ----------------------------------------------------------------------- init
-@pytest.mark.parametrize("model", ["vogels_abbott", "brunel", "brunel_with_plasticity"])
+@pytest.mark.parametrize("model", ["vogels_abbott", "brunel", "brunel_with_plasticity", "vogels_abbott_ns", "brunel_fixed",
+                                   "brunel_with_plasticity_a012"])
 def test_init_state_equals_oracle(model):
     # spice_test/cuda/snn.d.cpp:72-100: GPU init state == CPU init state at 0.0
     pops, conns = [100], [(0, 0, 0.1)]
@@ -100,11 +101,14 @@ def test_init_state_equals_oracle(model):
     assert net.num_neurons() == 100 and net.delay() == 15 and net.dt() == np.float32(1e-4)
     for a, b in zip(net.neurons(), ref.neurons()):
         assert bits_equal(a, b)
-    if model == "brunel_with_plasticity":
+    if model.startswith("brunel_with_plasticity"):
         e, _ = net.adj()
         valid = e != INT_MAX
         for a, b in zip(net.synapses(), ref.synapses()):
             assert bits_equal(a[valid], b[valid])
+    if model == "vogels_abbott_ns":  # V uniform in [-60, -50) mV, drawn per neuron
+        v = net.neurons()[0]
+        assert v.min() >= np.float32(-0.06) and v.max() < np.float32(-0.05) and len(np.unique(v)) > 90
 
 
 # ----------------------------------------------------------------------- dynamics
@@ -113,7 +117,7 @@ def check_neurons(model, got, want):
     V_RTOL relative (scale: the 20 mV threshold), since weights may differ by an ulp of
     expf between device and host."""
     for k, (a, b) in enumerate(zip(got, want)):
-        if model != "brunel_with_plasticity" or a.dtype != np.float32:
+        if not model.startswith("brunel_with_plasticity") or a.dtype != np.float32:
             assert bits_equal(a, b), f"{model}: neuron attribute {k} differs"
         else:
             err = np.max(np.abs(a.astype(np.float64) - b) / np.maximum(np.abs(b), 0.02))
@@ -184,6 +188,26 @@ def test_brunel_generated_graph(delay):
     run_parity("brunel", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], delay, 1000, 5, graph_seed=21)
 
 
+@pytest.mark.parametrize("model,pops,conns,delay,steps", [
+    ("vogels_abbott_ns", [4000], [(0, 0, 0.02)], 1, 1000),          # the VA configuration: 4,000 + 1,000, delay 1
+    ("vogels_abbott_ns", [4000], [(0, 0, 0.02)], 8, 1000),
+    ("brunel_fixed", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1000),
+    ("brunel_fixed", [1500, 1500], [(0, 1, 0.1), (1, 1, 0.1)], 3, 600),
+])
+def test_benchmark_configuration_models(model, pops, conns, delay, steps):
+    """The models with the benchmark configurations' constants, against the oracle's
+    restatement of the same constants: rasters identical every step, state bit for bit."""
+    run_parity(model, pops, conns, delay, steps, 11, graph_seed=12)
+
+
+def test_brunel_plus_a012_stdp_active():
+    """Brunel+ with A- = 0.012, in the small low-rate regime where weights change."""
+    net, ref = run_parity("brunel_with_plasticity_a012", [300, 300], [(0, 1, 0.1), (1, 1, 0.1)], 15, 3000, 7, graph_seed=5,
+                          check_w=True)
+    e, _ = net.adj()
+    assert len(np.unique(net.synapses()[0][e != INT_MAX])) > 10
+
+
 def test_synth_model():
     run_parity("synth", [3000], [(0, 0, 0.01)], 4, 300, 9, graph_seed=3)
 
@@ -207,12 +231,17 @@ POPULATIONS = {  # the models' populations: (first, last) as fractions of N
     "brunel_with_plasticity": [(0.0, 0.5), (0.5, 0.9), (0.9, 1.0)],
     "vogels_abbott": [(0.0, 0.8), (0.8, 1.0)],                      # exc, inh (vogels_abbott.h:78-84)
 }
+for _m in ("brunel_fixed", "brunel_with_plasticity_a012", "vogels_abbott_ns"):
+    POPULATIONS[_m] = POPULATIONS[_m.replace("_fixed", "").replace("_a012", "").replace("_ns", "")]
 
 
 @pytest.mark.parametrize("model,pops,conns,delay,seed,graph_seed", [
     ("brunel", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 2, 2),
     ("vogels_abbott", [4000], [(0, 0, 0.02)], 1, 1, 1337),
     ("brunel_with_plasticity", [300, 300], [(0, 1, 0.1), (1, 1, 0.1)], 15, 7, 5),
+    ("vogels_abbott_ns", [4000], [(0, 0, 0.02)], 1, 1, 1337),
+    ("brunel_fixed", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 2, 2),
+    ("brunel_with_plasticity_a012", [300, 300], [(0, 1, 0.1), (1, 1, 0.1)], 15, 7, 5),
 ])
 def test_fp64_accuracy_contract(model, pops, conns, delay, seed, graph_seed):
     """FP32 on the GPU against the FP64 oracle over 1 s of biological time (10,000 steps),
@@ -264,7 +293,7 @@ def test_fp64_accuracy_contract(model, pops, conns, delay, seed, graph_seed):
             assert rel <= 0.01, rates
         else:  # after the trajectories part: exactly the FP32 arithmetic's own drift
             assert rel == rel32, rates
-    if model == "brunel_with_plasticity":
+    if model.startswith("brunel_with_plasticity"):
         valid = e != INT_MAX
         assert np.max(np.abs(net.synapses()[0][valid] - f64.synapses()[0][valid])) <= W_ATOL_FP64
 
@@ -654,3 +683,30 @@ def test_restore_refuses_corrupted_checkpoints():
         Snn.restore(bad)
     q = Snn.restore(data)
     assert np.array_equal(p.step(out=True), q.step(out=True))
+
+
+def test_withheld_publication_ends_the_launch_with_a_timeout(monkeypatch):
+    """Failure detection inside one persistent launch: a tile that never publishes its steps
+    (a flag that nothing sets) makes the waits of every tile reading it run out; the launch
+    ends, the net reports SPK_ERR_DEVICE with ERR_TIMEOUT (4) in its error word, and the GPU
+    context stays usable for the next net."""
+    monkeypatch.setenv("SPK_TEST_WITHHOLD_TILE", "3")
+    monkeypatch.setenv("SPK_TEST_WAIT_LIMIT", "2000")
+    lay = Layout([10_000, 10_000], [(0, 1, 0.1), (1, 1, 0.1)])
+    net = Snn("brunel", lay, delay=15, seed=5, graph_seed=5)
+    assert net.info().persistent == 1
+    net.run(300)
+    with pytest.raises(spice_b200.SpiceError) as e:
+        net.sync()
+    assert e.value.code == spice_b200.ERR_DEVICE and "device error flag 4" in str(e.value)
+    net.close()
+    monkeypatch.delenv("SPK_TEST_WITHHOLD_TILE")
+    monkeypatch.delenv("SPK_TEST_WAIT_LIMIT")
+    ok = Snn("brunel", lay, delay=15, seed=5, graph_seed=5)
+    ref = oracle.OracleNet("brunel", [10_000, 10_000], [(0, 1, 0.1), (1, 1, 0.1)], delay=15, seed=5,
+                           edges=ok.adj()[0], width=ok.adj()[1])
+    ok.run(300)
+    for _ in range(300):
+        ref.step()
+    for a, b in zip(ok.neurons(), ref.neurons()):
+        assert bits_equal(a, b)

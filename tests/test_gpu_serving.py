@@ -58,6 +58,9 @@ def test_jobs_in_a_mix_equal_jobs_alone():
                 assert bits_equal(x, y), model
         st = srv.stats()
         assert st["done"] == len(JOBS) and st["bytes_in_use"] == 0 and st["ticks"] > 1
+        # the jobs ran together: some job started before another one ended
+        infos = [srv.info(j) for j in ids]
+        assert any(a.t_start < b.t_end and b.t_start < a.t_end for a in infos for b in infos if a is not b)
 
 
 def test_budget_bounds_concurrency_and_refuses_oversized_jobs():
@@ -113,3 +116,51 @@ def test_cancel_timeout_and_wait_limit():
         with pytest.raises(spice_b200.InvalidArgument):
             srv.info(late)
         assert srv.stats()["bytes_in_use"] == 0
+
+
+def test_injected_device_error_fails_one_job_only():
+    """A job whose net reports a device error (its error word set, as a kernel's bounded wait
+    that ran out sets it) fails with SPK_ERR_DEVICE; the jobs beside it, in the shared
+    launches and on their own streams, complete with the results they have alone."""
+    mix = [JOBS[0], JOBS[2], JOBS[4]]
+    with Server(budget_bytes=40 * GB, quantum=100) as srv:
+        ids = [srv.submit(m, Layout(p, c), steps, delay=d, seed=i + 1, graph_seed=i + 101)
+               for i, (m, p, c, d, steps) in enumerate(mix)]
+        victim = srv.submit("brunel", Layout([3000, 3000], [(0, 1, 0.1), (1, 1, 0.1)]), 5000, delay=15, seed=9)
+        for _ in range(600):  # running, so that its net exists
+            if srv.state(victim) == "running":
+                break
+            time.sleep(0.01)
+        srv.inject_device_error(victim)
+        srv.wait(timeout=300)
+        iv = srv.info(victim)
+        assert srv.state(victim) == "failed" and iv.error == spice_b200.ERR_DEVICE and b"device error flag 4" in iv.message
+        for i, (m, p, c, d, steps) in enumerate(mix):
+            assert srv.state(ids[i]) == "done", srv.info(ids[i]).message
+            for x, y in zip(srv.neurons(ids[i]), alone(m, p, c, d, steps, i + 1)):
+                assert bits_equal(x, y), m
+        assert srv.stats()["bytes_in_use"] == 0
+        with pytest.raises(spice_b200.InvalidArgument):
+            srv.inject_device_error(victim)  # finished
+
+
+SERVED = [  # the serving workload's shapes (bench.py serving_jobs): smallest and largest of each model
+    ("vogels_abbott", lambda n: ([n], [(0, 0, 0.02)]), 8, [7071, 100_000]),
+    ("brunel", lambda n: ([n // 2, n // 2], [(0, 1, 0.1), (1, 1, 0.1)]), 15, [4472, 63_245]),
+    ("brunel_with_plasticity", lambda n: ([n // 2, n // 2], [(0, 1, 0.1), (1, 1, 0.1)]), 15, [4472, 63_245]),
+]
+
+
+@pytest.mark.parametrize("tile_target", [0, 4, 37])
+def test_estimate_bounds_the_device_memory_a_net_holds(tile_target):
+    """The estimate the server admits jobs by is an upper bound of every net's device memory,
+    for each model, size and tiling of the serving mix, and of the mix test's jobs."""
+    cases = [(m, *shape(n), d) for m, shape, d, ns in SERVED for n in ns]
+    cases += [(m, p, c, d) for m, p, c, d, _ in JOBS]
+    for model, pops, conns, delay in cases:
+        lay = Layout(pops, conns)
+        est = spice_b200.estimate_bytes(model, lay, delay=delay, tile_target=tile_target)
+        net = Snn(model, lay, delay=delay, tile_target=tile_target)
+        held = net.info().device_bytes
+        net.close()
+        assert held <= est, (model, pops, tile_target, held, est)
