@@ -73,6 +73,8 @@ typedef struct spk_net_info
 	int persistent;        /* 1: spk_net_run advances the net in one cooperative launch */
 	int slice_pack;        /* window_flat slices: 8 (16-bit) or 12 (10-bit) indices per
 	                          16-byte vector; 0 for the other window kernels            */
+	int slot_vecs;         /* window_slots: 16-byte vectors per fixed (source, tile) slot;
+	                          0 when the net keeps variable slices                     */
 } spk_net_info;
 
 /* Message of the last failed call on this host thread ("" if none). */

@@ -70,6 +70,7 @@ class NetInfo(C.Structure):
         ("kernel_launches", C.c_uint64),
         ("persistent", C.c_int),
         ("slice_pack", C.c_int),
+        ("slot_vecs", C.c_int),
     ]
 
 

@@ -514,6 +514,8 @@ __device__ __forceinline__ void compact_step( net_params const & p, unsigned con
 {
 	int const slot_out = (int)( t % p.ring );
 	int * out = p.ring_ids + (long long)slot_out * p.n + d0;
+	// the step's summary record (nets with slots): count, then the first 31 ids
+	int * summ = p.summ ? p.summ + ( (long long)slot_out * p.ntiles + tile ) * 32 : nullptr;
 	int done = 0;
 	for( int w0 = 0; w0 < words; w0 += 32 )
 	{
@@ -526,11 +528,17 @@ __device__ __forceinline__ void compact_step( net_params const & p, unsigned con
 		{
 			int const b = __ffs( m ) - 1;
 			m &= m - 1;
-			out[off++] = d0 + ( w << 5 ) + b;
+			int const id = d0 + ( w << 5 ) + b;
+			if( summ && off < 31 ) summ[1 + off] = id;
+			out[off++] = id;
 		}
 		done += __shfl_sync( 0xffffffffu, incl, 31 );
 	}
-	if( lane == 0 ) p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
+	if( lane == 0 )
+	{
+		p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
+		if( summ ) summ[0] = done;
+	}
 	// every lane's ring writes, then the flag that publishes them
 	__threadfence();
 	__syncwarp();

@@ -72,6 +72,13 @@ struct net_params
 	long long * done_step;   // [ntiles] last step whose spikes the tile has published
 	int wait_limit;          // polls of a bounded wait before it gives up (WAIT_LIMIT)
 	int withhold_tile;       // failure-detection tests: this tile never publishes (-1: none)
+	// fixed slots (window_slots): S vectors per (source, tile with inputs), the index of
+	// every tile among the tiles with inputs (-1: none) and their number; spike summaries
+	// [ring][ntiles][32]: count and first 31 ids of every (step, tile)
+	uint4 const * slots;
+	int const * tile_in;
+	int tin, slot_vecs;
+	int * summ;
 };
 
 template <typename T>

@@ -8,6 +8,7 @@
 #include "flat.cuh"
 #include "models.cuh"
 #include "plastic.cuh"
+#include "slots.cuh"
 
 #include <spice/util/layout.h>
 #include <spice_b200.h>
@@ -378,6 +379,11 @@ tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 }
 } // namespace
 
+namespace
+{
+void summaries_from_ring( spk_net & net );
+}
+
 struct spk_net
 {
 	// owns `stream` (destroyed, or handed back to the device's stream_recycler if it came
@@ -433,6 +439,12 @@ struct spk_net
 	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
 	int pack = 8;           // slice indices per 16-byte vector: 8 (16-bit) or 12 (10-bit)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
+	// window_slots (10-bit nets whose slices fit fixed slots, section on slots in slots.cuh):
+	// slot_vecs > 0 selects it over window_flat; the slots, the tiles' indices among the
+	// tiles with inputs and the spike-summary ring
+	int slot_vecs = 0, tin = 0;
+	int slot_smem = 0; // dynamic shared memory of a window_slots launch
+	dbuf slot_data, tile_in, summ;
 	bool persistent = false; // run() as one cooperative window_flat launch (delay >= 6)
 	// failure-detection tests (SPK_TEST_WAIT_LIMIT, SPK_TEST_WITHHOLD_TILE at creation): a
 	// shorter bounded wait, and a tile that never publishes its steps so that the waits of
@@ -477,6 +489,11 @@ struct spk_net
 		p.done_step = done_step.as<long long>();
 		p.wait_limit = wait_limit;
 		p.withhold_tile = withhold_tile;
+		p.slots = slot_data.as<uint4 const>();
+		p.tile_in = tile_in.as<int const>();
+		p.tin = tin;
+		p.slot_vecs = slot_vecs;
+		p.summ = summ.as<int>();
 		return p;
 	}
 
@@ -484,7 +501,8 @@ struct spk_net
 	{
 		size_t b = edges.bytes + pivots.bytes + tile_first.bytes + ring_ids.bytes + ring_cnt.bytes + clock.bytes + dt_ring.bytes + err.bytes +
 		           conns_dev.bytes + gather_ids.bytes + gather_cnt.bytes + cursor.bytes + gather_done.bytes + rec_ids.bytes +
-		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + done_step.bytes;
+		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + done_step.bytes +
+		           slot_data.bytes + tile_in.bytes + summ.bytes;
 		for( auto const & a : attr ) b += a.bytes;
 		return b;
 	}
@@ -494,7 +512,7 @@ struct spk_net
 
 	int window_smem() const
 	{
-		if( flat ) return flat_smem;
+		if( flat ) return slot_vecs ? slot_smem : flat_smem;
 		int const classes = this->classes();
 		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
 		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
@@ -548,11 +566,20 @@ struct spk_net
 				flat_smem = std::min( flat_smem, optin - (int)fb.sharedSizeBytes );
 				set_smem_limit( (void const *)spk::window_flat<Model>, device, flat_smem );
 				set_smem_limit( (void const *)spk::window_flat_batch<Model>, device, flat_smem );
+				cudaFuncAttributes fs{}, fsb{};
+				CK( cudaFuncGetAttributes( &fs, spk::window_slots<Model> ) );
+				CK( cudaFuncGetAttributes( &fsb, spk::window_slots_batch<Model> ) );
+				slot_smem = optin - (int)std::max( fs.sharedSizeBytes, fsb.sharedSizeBytes );
+				set_smem_limit( (void const *)spk::window_slots<Model>, device, slot_smem );
+				set_smem_limit( (void const *)spk::window_slots_batch<Model>, device, slot_smem );
 				// one launch for a whole run: every tile's CTA resident at once (cooperative
 				// launch), and the step pipeline never waits on a step not yet simulated
 				int coop = 0, per_sm = 0;
 				CK( cudaDeviceGetAttribute( &coop, cudaDevAttrCooperativeLaunch, device ) );
-				CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_flat<Model>, tc.threads, flat_smem ) );
+				if( slot_vecs )
+					CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_slots<Model>, tc.threads, slot_smem ) );
+				else
+					CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_flat<Model>, tc.threads, flat_smem ) );
 				char const * pers = getenv( "SPK_PERSIST" );
 				persistent = coop && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
 				return;
@@ -584,6 +611,10 @@ struct spk_net
 		{
 			auto const q = plast.params();
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
+		}
+		else if( flat && slot_vecs )
+		{
+			if constexpr( spk::is_flat_model<Model> ) spk::window_slots<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
 		}
 		else if( flat )
 			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
@@ -674,6 +705,11 @@ struct spk_net
 		ring_ids.swap( ids );
 		ring_cnt.swap( cnt );
 		ring_slots = slots;
+		if( slot_vecs )
+		{
+			summaries_from_ring( *this );
+			CK( cudaStreamSynchronize( stream ) );
+		}
 		if( graph ) cudaGraphExecDestroy( graph ); // captured the old ring
 		graph = nullptr;
 	}
@@ -702,13 +738,15 @@ struct spk_net
 		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
 		{
 			auto p = params();
-			// the step pipeline looks five steps ahead, which needs delay >= 6; shorter delays
-			// run every step on the synchronous path (each step waits for the steps it reads)
-			if( delay < 6 ) p.flat_sync = 1;
-			int smem = flat_smem;
+			// window_flat's step pipeline looks five steps ahead, which needs delay >= 6;
+			// shorter delays run every step on the synchronous path (each step waits for the
+			// steps it reads). window_slots looks three steps ahead (its nets have delay >= 4).
+			if( !slot_vecs && delay < 6 ) p.flat_sync = 1;
+			int smem = slot_vecs ? slot_smem : flat_smem;
 			float d = dt;
 			void * args[] = { &p, &L, &d, &smem };
-			CK( cudaLaunchCooperativeKernel( (void const *)spk::window_flat<Model>, dim3( tc.ntiles ), dim3( tc.threads ), args, (size_t)smem, stream ) );
+			void const * kernel = slot_vecs ? (void const *)spk::window_slots<Model> : (void const *)spk::window_flat<Model>;
+			CK( cudaLaunchCooperativeKernel( kernel, dim3( tc.ntiles ), dim3( tc.threads ), args, (size_t)smem, stream ) );
 		}
 	}
 	void launch_persistent( int L )
@@ -1050,6 +1088,77 @@ void fill_slices( spk_net & net, sbuf const & bases )
 	}
 }
 
+template <typename Model>
+void fill_slots( spk_net & net )
+{
+	if constexpr( Model::neuron::input_classes > 0 )
+	{
+		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
+		spk::slot_fill<Model><<<blocks, 256, 0, net.stream>>>(
+		    (int)net.n, (int)net.width, net.tc.ntiles, net.edges.as<int>(), net.pivots.as<unsigned>(), net.tile_first.as<int>(),
+		    net.tile_in.as<int>(), net.tin, net.slot_vecs, net.slot_data.as<uint4>() );
+		CK( cudaGetLastError() );
+	}
+}
+
+// the spike-summary ring of a slotted net, rebuilt from its spike ring (after a restore or
+// when the ring grows)
+void summaries_from_ring( spk_net & net )
+{
+	if( !net.slot_vecs ) return;
+	net.summ.alloc( (size_t)net.ring_slots * net.tc.ntiles * spk::SUM_W * 4, net.mem() );
+	long long const warps = (long long)net.ring_slots * net.tc.ntiles;
+	spk::summ_from_ring<<<(int)( ( warps * 32 + 255 ) / 256 ), 256, 0, net.stream>>>(
+	    net.ring_ids.as<int>(), net.ring_cnt.as<unsigned>(), (int)net.n, net.tc.ntiles, net.ring_slots, net.tile_first.as<int>(),
+	    net.summ.as<int>() );
+	CK( cudaGetLastError() );
+}
+
+// Fixed slots (window_slots) instead of variable slices: for 10-bit nets with delay >= 4
+// whose longest slice fits 8 vectors, when the slots are at least half full on average
+// (`vectors` = the variable slices' vectors) and a step's arrivals fit the shared memory.
+// SPK_SLOTS=0 keeps the variable slices, SPK_SLOTS=1 takes slots whenever they fit.
+bool plan_slots( spk_net & net, unsigned long long vectors )
+{
+	net.slot_vecs = 0;
+	net.tin = 0;
+	net.slot_data.reset();
+	net.tile_in.reset();
+	net.summ.reset();
+	char const * env = getenv( "SPK_SLOTS" );
+	bool const off = env && !strcmp( env, "0" ), force = env && !strcmp( env, "1" );
+	int const nt = net.tc.ntiles;
+	if( off || net.pack != 12 || net.delay < 4 || net.width == 0 ) return false;
+	std::vector<int> in( nt ), idx( nt, -1 );
+	CK( cudaMemcpyAsync( in.data(), net.tile_inputs.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
+	sbuf mx( 4, net.stream, net.device );
+	CK( cudaMemsetAsync( mx.p, 0, 4, net.stream ) );
+	spk::slice_max<<<4 * net.sms, 256, 0, net.stream>>>( (int)net.n, nt, net.pivots.as<unsigned>(), mx.as<unsigned>() );
+	CK( cudaGetLastError() );
+	unsigned longest = 0;
+	CK( cudaMemcpyAsync( &longest, mx.p, 4, cudaMemcpyDeviceToHost, net.stream ) );
+	CK( cudaStreamSynchronize( net.stream ) );
+	int tin = 0;
+	for( int j = 0; j < nt; j++ )
+		if( in[j] ) idx[j] = tin++;
+	int S = 2;
+	while( S < 8 && (unsigned)S * 12 < longest ) S *= 2;
+	if( tin == 0 || (unsigned)S * 12 < longest ) return false;
+	double const full = (double)vectors / ( (double)net.n * tin * S );
+	spk::slot_geom const g = spk::slot_layout( net.classes(), net.neuron_attrs(), net.flat_tmax, nt, S, net.slot_smem );
+	if( g.ecap < spk::SLOT_MIN_ECAP || (size_t)2 * g.ecap * S * 16 < spk::slot_direct_scratch( nt ) ) return false;
+	if( !force && full < 0.5 ) return false;
+	net.slot_vecs = S;
+	net.tin = tin;
+	net.tile_in.alloc( (size_t)nt * 4, net.mem() );
+	CK( cudaMemcpyAsync( net.tile_in.p, idx.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, net.stream ) );
+	net.slot_data.alloc( (size_t)net.n * tin * S * 16, net.mem() );
+	dispatch( net.model, [&]( auto tag ) { fill_slots<typename decltype( tag )::type>( net ); } );
+	summaries_from_ring( net );
+	CK( cudaStreamSynchronize( net.stream ) ); // idx is freed on return
+	return true;
+}
+
 // the tile-major slices of window_flat, from the ELL rows and their pivots
 void build_slices( spk_net & net )
 {
@@ -1080,6 +1189,14 @@ void build_slices( spk_net & net )
 	net.flat_sync = sync && !strcmp( sync, "1" );
 	net.done_step.alloc( (size_t)nt * sizeof( long long ), net.mem() );
 	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
+	if( plan_slots( net, all ) )
+	{
+		net.slice_rec.reset();
+		net.slices.reset();
+		CK( cudaStreamSynchronize( net.stream ) );
+		net.configure(); // the persistent launch of window_slots
+		return;
+	}
 	net.slices.alloc( std::max<size_t>( (size_t)all * 16, 16 ), net.mem() );
 	CK( cudaMemcpyAsync( bases.p, base.data(), (size_t)n * 8, cudaMemcpyHostToDevice, net.stream ) );
 	dispatch( net.model, [&]( auto tag ) { fill_slices<typename decltype( tag )::type>( net, bases ); } );
@@ -1209,6 +1326,14 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	{
 		b.push_back( (double)n * T * 8 );
 		b.push_back( 16.0 * ( std::ceil( syn / pack ) + std::min( (double)n * T, syn ) ) );
+		if( pack == 12 && delay >= 4 )
+		{
+			// fixed slots, taken when at least half full: at most twice the slices' vectors
+			// (built beside the slice records), and the spike-summary ring
+			b.push_back( 16.0 * ( std::ceil( syn / pack ) + std::min( (double)n * T, syn ) ) );
+			b.push_back( 2.0 * delay * T * spk::SUM_W * 4 );
+			b.push_back( (double)T * 4 );
+		}
 		b.push_back( (double)T * 8 );
 		b.push_back( (double)T * 4 );
 	}
@@ -1463,7 +1588,7 @@ struct spk_batch
 	};
 	int device = 0;
 	std::vector<spk_net *> nets;
-	group groups[spk::MODEL_COUNT]; // by model id (models without plasticity only)
+	group groups[2 * spk::MODEL_COUNT]; // by model id and kernel (window_flat, window_slots)
 
 	~spk_batch()
 	{
@@ -1480,11 +1605,14 @@ struct spk_batch
 	static bool shared( spk_net const & net ) { return net.flat && !plastic_of( net.model ); }
 
 	template <typename Model>
-	static void launch_model( group & g, int4 const * jobs, int njobs, int smem )
+	static void launch_model( group & g, int4 const * jobs, int njobs, int smem, bool slotted )
 	{
 		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
 		{
-			spk::window_flat_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
+			if( slotted )
+				spk::window_slots_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
+			else
+				spk::window_flat_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
 			CK( cudaGetLastError() );
 		}
 	}
@@ -1560,12 +1688,13 @@ struct spk_batch
 			g.c_jobs = g.h_jobs;
 			g.drop_graph();
 		}
-		int const smem = gn[0]->flat_smem;
+		bool const slotted = gn[0]->slot_vecs > 0;
+		int const smem = slotted ? gn[0]->slot_smem : gn[0]->flat_smem;
 		auto launch_all = [&] {
 			for( auto const & l : launches )
 			{
 				int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
-				dispatch( model, [&]( auto tag ) { launch_model<typename decltype( tag )::type>( g, jobs, l.second, smem ); } );
+				dispatch( model, [&]( auto tag ) { launch_model<typename decltype( tag )::type>( g, jobs, l.second, smem, slotted ); } );
 			}
 		};
 		// the rounds as one CUDA graph, captured once per job table and round sequence and
@@ -1603,21 +1732,22 @@ struct spk_batch
 	{
 		// nets outside window_flat (plastic ones) run their own windows on their own
 		// streams, concurrently with the shared launches
-		std::vector<spk_net *> gn[spk::MODEL_COUNT];
-		std::vector<unsigned long long> gc[spk::MODEL_COUNT];
+		std::vector<spk_net *> gn[2 * spk::MODEL_COUNT];
+		std::vector<unsigned long long> gc[2 * spk::MODEL_COUNT];
 		for( size_t i = 0; i < which.size(); i++ )
 		{
 			if( counts[i] == 0 ) continue;
 			if( shared( *which[i] ) )
 			{
-				gn[which[i]->model].push_back( which[i] );
-				gc[which[i]->model].push_back( counts[i] );
+				int const gi = 2 * which[i]->model + ( which[i]->slot_vecs ? 1 : 0 );
+				gn[gi].push_back( which[i] );
+				gc[gi].push_back( counts[i] );
 			}
 			else
 				which[i]->run( counts[i] );
 		}
-		for( int m = 0; m < spk::MODEL_COUNT; m++ )
-			if( !gn[m].empty() ) run_group( groups[m], m, gn[m], gc[m] );
+		for( int m = 0; m < 2 * spk::MODEL_COUNT; m++ )
+			if( !gn[m].empty() ) run_group( groups[m], m / 2, gn[m], gc[m] );
 	}
 };
 
@@ -1990,6 +2120,7 @@ int spk_net_get_info( spk_net * net, spk_net_info * out )
 		out->kernel_launches = net->kernel_launches;
 		out->persistent = net->persistent ? 1 : 0;
 		out->slice_pack = net->flat ? net->pack : 0;
+		out->slot_vecs = net->slot_vecs;
 	} );
 }
 
@@ -2161,6 +2292,7 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		for( auto const & x : ckpt_plastic( *net ) )
 			if( x.second->bytes )
 				CK( cudaMemcpyAsync( x.second->p, find( x.first, x.second->bytes ), x.second->bytes, cudaMemcpyHostToDevice, net->stream ) );
+		summaries_from_ring( *net ); // slotted nets: the summaries of the restored ring
 		CK( cudaStreamSynchronize( net->stream ) );
 		net->steps = net->launched = h.steps;
 		net->configure();
@@ -2358,7 +2490,8 @@ int spk_batch_add( spk_batch * b, spk_net * net )
 		require( net->batch == nullptr, "the net belongs to a batch already" );
 		if( spk_batch::shared( *net ) )
 			for( auto * o : b->nets )
-				require( !spk_batch::shared( *o ) || o->flat_smem == net->flat_smem, "nets of a batch share one kernel configuration" );
+				require( !spk_batch::shared( *o ) || ( o->flat_smem == net->flat_smem && o->slot_smem == net->slot_smem ),
+				         "nets of a batch share one kernel configuration" );
 		b->nets.push_back( net );
 		net->batch = b;
 	} );

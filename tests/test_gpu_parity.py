@@ -730,3 +730,85 @@ def test_withheld_publication_ends_the_launch_with_a_timeout(monkeypatch):
         ref.step()
     for a, b in zip(ok.neurons(), ref.neurons()):
         assert bits_equal(a, b)
+
+
+# ----------------------------------------------------------------------- fixed slots
+SLOT_NETS = [
+    ("brunel", [20_000, 20_000], [(0, 1, 0.05), (1, 1, 0.05)], 15, 600),   # the pipeline, persistent
+    ("vogels_abbott", [30_000], [(0, 0, 0.02)], 8, 400),
+    ("synth", [150_000], [(0, 0, 16 / 150_000)], 4, 300),                 # delay 4: the shortest look-ahead
+    ("synth", [150_000], [(0, 0, 0.01)], 6, 100),                         # 750 arrivals a step, slots of 2 vectors
+    ("brunel", [60_000, 4_000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 200),    # Poisson tiles of > 31 spikes: direct steps
+]
+
+
+@pytest.mark.parametrize("model,pops,conns,delay,steps", SLOT_NETS)
+def test_slots_match_variable_slices(model, pops, conns, delay, steps, monkeypatch):
+    """window_slots (fixed slots, spike summaries) against window_flat (variable slices) on
+    the same net: persistent recording runs, then windowed steps, bit for bit."""
+    layout = Layout(pops, conns)
+    monkeypatch.setenv("SPK_SLOTS", "1")
+    a = Snn(model, layout, delay=delay, seed=3, graph_seed=9)
+    monkeypatch.setenv("SPK_SLOTS", "0")
+    b = Snn(model, layout, delay=delay, seed=3, graph_seed=9)
+    assert a.info().slot_vecs > 0 and b.info().slot_vecs == 0
+    ca, ia = a.run_record(steps, cap=sum(pops) * steps // 4)
+    cb, ib = b.run_record(steps, cap=sum(pops) * steps // 4)
+    assert ca.sum() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+    for k in range(2 * delay + 3):  # windowed launches after the persistent one
+        assert np.array_equal(a.step(out=True), b.step(out=True)), k
+    a.run(3 * delay + 1)
+    b.run(3 * delay + 1)
+    for x, y in zip(a.neurons(), b.neurons()):
+        assert bits_equal(x, y)
+
+
+def test_slots_against_the_oracle(monkeypatch):
+    """A slotted Brunel net against the oracle, spike by spike, and its persistent run."""
+    monkeypatch.setenv("SPK_SLOTS", "1")
+    net, ref = run_parity("brunel", [3000, 3000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 700, 4, graph_seed=14)
+    assert net.info().slot_vecs > 0
+    counts, ids = net.run_record(500)
+    o = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    for k in range(500):
+        assert np.array_equal(ids[o[k]:o[k + 1]], ref.step()), k
+    check_neurons("brunel", net.neurons(), ref.neurons())
+
+
+def test_slotted_nets_in_a_batch_and_restored(monkeypatch):
+    """window_slots_batch (slotted nets in shared launches, beside nets with variable
+    slices) and a slotted net's checkpoint (its summaries rebuilt from the spike ring)."""
+    nets = [("brunel", [10_000, 10_000], [(0, 1, 0.1), (1, 1, 0.1)], 15), ("vogels_abbott", [20_000], [(0, 0, 0.02)], 8),
+            ("synth", [100_000], [(0, 0, 30 / 100_000)], 6)]
+    batch = spice_b200.Batch()
+    alone, batched = [], []
+    for i, (model, pops, conns, delay) in enumerate(nets):
+        for slots in ("1", "0"):
+            monkeypatch.setenv("SPK_SLOTS", slots)
+            a = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7)
+            b = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7)
+            b.set_tile_target(24 + 10 * i)
+            assert (b.info().slot_vecs > 0) == (slots == "1")
+            batch.add(b)
+            alone.append(a)
+            batched.append(b)
+    batch.run(77)
+    batch.run(77)
+    for a in alone:
+        a.run(154)
+    for a, b in zip(alone, batched):
+        for x, y in zip(a.neurons(), b.neurons()):
+            assert bits_equal(x, y)
+        for k in range(3):
+            assert np.array_equal(a.step(out=True), b.step(out=True)), k
+    batch.close()
+    s = alone[0]
+    assert s.info().slot_vecs > 0
+    s.run_record(300, cap=20_000 * 300)  # an enlarged ring
+    r = Snn.restore(s.checkpoint())
+    assert r.info().slot_vecs > 0
+    ca, ia = s.run_record(100, cap=20_000 * 100)
+    cb, ib = r.run_record(100, cap=20_000 * 100)
+    assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
