@@ -142,9 +142,42 @@ int spk_net_create_ex(
     int device,
     int tile_target );
 
+/* Build choices of a net. A field at -1 is chosen automatically; for such a field the
+ * environment variable named beside it, where set, overrides the automatic choice (a test
+ * hook: an explicit field value always wins). Results never depend on these choices: they
+ * select kernels and data layouts that all compute the same integer spike counts. */
+typedef struct spk_net_options
+{
+    int tile_target; /* window_flat tiles: about this many; 0 = one per SM */
+    int kernel;      /* SPK_KERNEL: 0 = window kernels (window_flat where the model allows), 1 = per-step kernels ("direct") */
+    int slice_bits;  /* SPK_PACK: 10 = 10-bit target indices where every index fits (12 to a vector), 16 = 16-bit (8 to a vector) */
+    int tiling;      /* SPK_TILES: 0 = tiles balanced by per-neuron cost, 1 = equal tiles ("uniform") */
+    int persistent;  /* SPK_PERSIST: 1 = one cooperative launch per run when every tile's CTA is resident, 0 = windowed launches */
+    int pipelined;   /* SPK_FLAT_SYNC (inverted): 1 = window_flat's step pipeline, 0 = every step synchronous */
+    int slots;       /* SPK_SLOTS: 1 = fixed slots (window_slots) where they fit, 0 = variable slices (the automatic choice) */
+} spk_net_options;
+
+/* Every field automatic (-1), tile_target 0. */
+void spk_net_options_init( spk_net_options * opts );
+
+/* spk_net_create with explicit build choices (`opts` null: all automatic). */
+int spk_net_create_opts(
+    spk_net ** out,
+    int model,
+    spk_layout_desc const * desc,
+    float dt,
+    int delay,
+    uint64_t seed,
+    uint64_t graph_seed,
+    int device,
+    spk_net_options const * opts );
+
 /* Upper estimate of the device memory (bytes) a net of this model, layout, delay and tile
  * target would hold once built: what a server admits against its memory budget. */
 int spk_net_estimate_bytes( int model, spk_layout_desc const * desc, int delay, int device, int tile_target, uint64_t * out_bytes );
+
+/* spk_net_estimate_bytes for a net built with `opts` (null: all automatic). */
+int spk_net_estimate_bytes_opts( int model, spk_layout_desc const * desc, int delay, int device, spk_net_options const * opts, uint64_t * out_bytes );
 
 /* cuda::snn<Model>(adj, width, dt, delay) (spice/cuda/snn.h:26-32, spice/cuda/snn.d.cpp:167-199):
  * imports an ELL adjacency (num_neurons x width int32, rows ascending, INT_MAX padded,

@@ -97,6 +97,42 @@ class ServerStats(C.Structure):  # spk_server_stats
 
 JOB_STATES = ("queued", "running", "done", "failed", "cancelled", "timeout", "refused")
 
+class _NetOptions(C.Structure):
+    _fields_ = [(f, C.c_int) for f in ("tile_target", "kernel", "slice_bits", "tiling", "persistent", "pipelined", "slots")]
+
+
+# build choices (spk_net_options): name -> (field, {value: int})
+_OPTION_VALUES = {
+    "kernel": {"window": 0, "direct": 1},
+    "slice_bits": {10: 10, 16: 16},
+    "tiling": {"balanced": 0, "uniform": 1},
+    "persistent": {False: 0, True: 1},
+    "pipelined": {False: 0, True: 1},
+    "slots": {False: 0, True: 1},
+}
+
+
+def net_options(tile_target=0, **choices):
+    """spk_net_options from keyword choices (kernel="window"|"direct", slice_bits=10|16,
+    tiling="balanced"|"uniform", persistent=bool, pipelined=bool, slots=bool); a choice
+    left out is automatic."""
+    o = _NetOptions()
+    library().spk_net_options_init(C.byref(o))
+    if int(tile_target) < 0:
+        raise InvalidArgument(ERR_INVALID, "tile target must be >= 0")
+    o.tile_target = int(tile_target)
+    for k, v in choices.items():
+        if k not in _OPTION_VALUES:
+            raise InvalidArgument(ERR_INVALID, f"unknown net option {k!r}")
+        if v is None:
+            continue
+        table = _OPTION_VALUES[k]
+        if v not in table:
+            raise InvalidArgument(ERR_INVALID, f"net option {k}={v!r} is not one of {list(table)}")
+        setattr(o, k, table[v])
+    return o
+
+
 _lib = None
 
 
@@ -134,6 +170,9 @@ def library():
         "spk_net_restore": (I, [P(VP), VP, U64, I]),
         "spk_net_create_ex": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I, I]),
         "spk_net_estimate_bytes": (I, [I, P(_LayoutDesc), I, I, I, P(U64)]),
+        "spk_net_options_init": (None, [P(_NetOptions)]),
+        "spk_net_create_opts": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I, P(_NetOptions)]),
+        "spk_net_estimate_bytes_opts": (I, [I, P(_LayoutDesc), I, I, P(_NetOptions), P(U64)]),
         "spk_batch_run_nets": (I, [VP, I, P(VP), P(U64)]),
         "spk_server_create": (I, [P(VP), I, U64, U64]),
         "spk_server_submit": (I, [VP, I, P(_LayoutDesc), F, I, U64, U64, U64, C.c_double, P(U64)]),
@@ -234,12 +273,14 @@ class Snn:
     """One simulated network on one GPU: the reference's cuda::snn<Model>.
 
     Snn(model, layout, dt, delay=1, seed=1, graph_seed=1337)   generate the graph on device
-                                                                (tile_target: tiles for a GPU shared with others)
+                                                                (tile_target: tiles for a GPU shared with others;
+                                                                options: build choices, see net_options)
     Snn(model, adj=(edges, width), dt=..., delay=...)           import an ELL adjacency
     Snn.from_state(model, edges, width, neurons, synapses, ...)  conversion constructor
     """
 
-    def __init__(self, model, layout=None, dt=1e-4, delay=1, seed=1, graph_seed=1337, device=0, adj=None, tile_target=0):
+    def __init__(self, model, layout=None, dt=1e-4, delay=1, seed=1, graph_seed=1337, device=0, adj=None, tile_target=0,
+                 options=None):
         lib = library()
         self.model = model if isinstance(model, str) else MODEL_NAMES[int(model)]
         m = MODELS[self.model]
@@ -255,8 +296,9 @@ class Snn:
             if layout is None:
                 raise InvalidArgument(ERR_INVALID, "layout or adj required")
             d = layout.desc()
-            _check(lib.spk_net_create_ex(C.byref(self._h), m, C.byref(d), float(dt), int(delay), int(seed), int(graph_seed),
-                                         int(device), int(tile_target)))
+            o = net_options(tile_target, **(options or {}))
+            _check(lib.spk_net_create_opts(C.byref(self._h), m, C.byref(d), float(dt), int(delay), int(seed), int(graph_seed),
+                                           int(device), C.byref(o)))
         self._ndt, self._sdt = model_attrs(self.model)
 
     @classmethod
@@ -444,12 +486,13 @@ class Batch:
         self.close()
 
 
-def estimate_bytes(model, layout, delay=1, device=0, tile_target=0):
+def estimate_bytes(model, layout, delay=1, device=0, tile_target=0, options=None):
     """Upper estimate of the device memory a net of this model and layout would hold."""
     m = MODELS[model] if isinstance(model, str) else int(model)
     d = layout.desc()
     out = C.c_uint64()
-    _check(library().spk_net_estimate_bytes(m, C.byref(d), int(delay), int(device), int(tile_target), C.byref(out)))
+    o = net_options(tile_target, **(options or {}))
+    _check(library().spk_net_estimate_bytes_opts(m, C.byref(d), int(delay), int(device), C.byref(o), C.byref(out)))
     return out.value
 
 

@@ -510,7 +510,8 @@ __device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2
 // ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
 // per round, a warp scan of their counts gives every word's offset; then the step is
 // published to the other tiles
-__device__ __forceinline__ void compact_step( net_params const & p, unsigned const * bits, int words, int d0, int tile, long long t, int lane )
+__device__ __forceinline__ void compact_step(
+    net_params const & p, unsigned const * bits, int words, int d0, int tile, long long t, int lane, bool publish = true )
 {
 	int const slot_out = (int)( t % p.ring );
 	int * out = p.ring_ids + (long long)slot_out * p.n + d0;
@@ -539,7 +540,9 @@ __device__ __forceinline__ void compact_step( net_params const & p, unsigned con
 		p.ring_cnt[(long long)slot_out * p.ntiles + tile] = (unsigned)done;
 		if( summ ) summ[0] = done;
 	}
-	// every lane's ring writes, then the flag that publishes them
+	// every lane's ring writes, then the flag that publishes them (and every step before:
+	// a caller may publish only every few steps)
+	if( !publish ) return;
 	__threadfence();
 	__syncwarp();
 	if( lane == 0 && tile != p.withhold_tile ) publish_step( p, tile, t );

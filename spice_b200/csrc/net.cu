@@ -384,6 +384,48 @@ namespace
 void summaries_from_ring( spk_net & net );
 }
 
+// A net's build choices: spk_net_options with every automatic field resolved (the
+// environment's test overrides applied to automatic fields only).
+struct build_opts
+{
+	int tile_target = 0;   // 0: one tile per SM
+	bool direct = false;   // per-step kernels instead of the window kernels
+	bool pack16 = false;   // 16-bit slice indices even where 10-bit ones fit
+	bool uniform = false;  // equal tiles instead of cost-balanced ones
+	bool windowed = false; // no persistent launch
+	bool flat_sync = false; // window_flat without its step pipeline
+	int slots = 0;         // 0: variable slices; 1: fixed slots where they fit; 2, 4, 8: exactly
+	                       // these slots (a restored slotted net)
+};
+
+build_opts resolve_opts( spk_net_options const * o )
+{
+	spk_net_options d;
+	spk_net_options_init( &d );
+	if( o ) d = *o;
+	require( d.tile_target >= 0, "tile target must be >= 0" );
+	auto env_is = []( char const * name, char const * value ) {
+		char const * e = getenv( name );
+		return e && !strcmp( e, value );
+	};
+	auto pick = [&]( int field, char const * name, char const * on, char const * off, bool dflt ) {
+		if( field >= 0 ) return field != 0;
+		if( env_is( name, on ) ) return true;
+		if( env_is( name, off ) ) return false;
+		return dflt;
+	};
+	require( d.slice_bits == -1 || d.slice_bits == 10 || d.slice_bits == 16, "slice_bits must be 10 or 16" );
+	build_opts r;
+	r.tile_target = d.tile_target;
+	r.direct = pick( d.kernel, "SPK_KERNEL", "direct", "window", false );
+	r.pack16 = d.slice_bits >= 0 ? d.slice_bits == 16 : env_is( "SPK_PACK", "16" );
+	r.uniform = pick( d.tiling, "SPK_TILES", "uniform", "balanced", false );
+	r.windowed = !pick( d.persistent, "SPK_PERSIST", "1", "0", true );
+	r.flat_sync = !pick( d.pipelined, "SPK_FLAT_SYNC", "0", "1", true );
+	r.slots = pick( d.slots, "SPK_SLOTS", "1", "0", false ) ? 1 : 0;
+	return r;
+}
+
 struct spk_net
 {
 	// owns `stream` (destroyed, or handed back to the device's stream_recycler if it came
@@ -406,6 +448,7 @@ struct spk_net
 	int model = 0;
 	int device = 0;
 	int sms = 148;
+	build_opts opts; // build choices (resolved spk_net_options)
 	cudaStream_t stream = nullptr;
 	cudaMemPool_t pool = nullptr; // null: cudaMalloc; else the net's buffers come from this pool on `stream`
 	long long n = 0, width = 0;
@@ -436,7 +479,7 @@ struct spk_net
 	int flat_smem = 0;   // dynamic shared memory of a window_flat launch
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
-	int flat_sync = 0;      // window_flat without its step pipeline (SPK_FLAT_SYNC=1)
+	int flat_sync = 0;      // window_flat without its step pipeline (opts.flat_sync)
 	int pack = 8;           // slice indices per 16-byte vector: 8 (16-bit) or 12 (10-bit)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
 	// window_slots (10-bit nets whose slices fit fixed slots, section on slots in slots.cuh):
@@ -580,8 +623,7 @@ struct spk_net
 					CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_slots<Model>, tc.threads, slot_smem ) );
 				else
 					CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, spk::window_flat<Model>, tc.threads, flat_smem ) );
-				char const * pers = getenv( "SPK_PERSIST" );
-				persistent = coop && (long long)per_sm * sms >= tc.ntiles && !( pers && !strcmp( pers, "0" ) );
+				persistent = coop && (long long)per_sm * sms >= tc.ntiles && !opts.windowed;
 				return;
 			}
 		// the limit is per kernel, shared by every net: set it to all a CTA can have, so a
@@ -740,7 +782,7 @@ struct spk_net
 			auto p = params();
 			// window_flat's step pipeline looks five steps ahead, which needs delay >= 6;
 			// shorter delays run every step on the synchronous path (each step waits for the
-			// steps it reads). window_slots looks three steps ahead (its nets have delay >= 4).
+			// steps it reads). window_slots looks five steps ahead (its nets have delay >= 7).
 			if( !slot_vecs && delay < 6 ) p.flat_sync = 1;
 			int smem = slot_vecs ? slot_smem : flat_smem;
 			float d = dt;
@@ -939,7 +981,8 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 // = the SM count for a net alone; fewer for a net that shares the GPU in a batch): the
 // tiles' first neurons and the shared-memory span of the largest tile with inputs; false
 // if the net does not fit window_flat.
-bool plan_flat( int model, int device, long long n, std::vector<cost_segment> const & segs, int target, std::vector<int> & first, int & span, int & pack )
+bool plan_flat(
+    int model, int device, long long n, std::vector<cost_segment> const & segs, int target, build_opts const & o, std::vector<int> & first, int & span, int & pack )
 {
 	int optin = 0;
 	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
@@ -952,8 +995,7 @@ bool plan_flat( int model, int device, long long n, std::vector<cost_segment> co
 	// tiles without inputs keep only their neuron state and fired bits
 	int const tmax_free = (int)std::max<long long>( tmax, ( ( optin - 4096LL ) * 32 / ( 32LL * 4 * attrs + 8 ) ) / 32 * 32 );
 	if( tmax < 128 ) return false;
-	char const * tiling = getenv( "SPK_TILES" );
-	bool const uniform = tiling && !strcmp( tiling, "uniform" );
+	bool const uniform = o.uniform;
 	auto cut = [&]( int tmax_in ) {
 		return uniform ? uniform_tiles( n, std::min( tmax_in, 1024 ) ) : balanced_tiles( segs, n, std::max( 1, target ), tmax_in, tmax_free );
 	};
@@ -974,11 +1016,10 @@ bool plan_flat( int model, int device, long long n, std::vector<cost_segment> co
 	span = input_span( first, tmax );
 	// 10-bit slices (twelve indices per vector instead of eight) when every counter index
 	// fits below SLICE_PAD10: tiles with inputs capped at (SLICE_PAD10 - 1) / classes
-	// neurons, taken if that needs no more tiles (SPK_PACK=16 keeps 16-bit slices)
+	// neurons, taken if that needs no more tiles (o.pack16 keeps 16-bit slices)
 	pack = 8;
-	char const * pk = getenv( "SPK_PACK" );
 	int const cap10 = (int)( ( spk::SLICE_PAD10 - 1 ) / std::max( 1, classes ) );
-	if( !( pk && !strcmp( pk, "16" ) ) && cap10 >= 128 )
+	if( !o.pack16 && cap10 >= 128 )
 	{
 		if( (long long)classes * span < (long long)spk::SLICE_PAD10 )
 			pack = 12;
@@ -1002,7 +1043,7 @@ bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int tar
 {
 	std::vector<int> first;
 	int span = 0, pack = 8;
-	if( !plan_flat( net.model, net.device, net.n, segs, target, first, span, pack ) ) return false;
+	if( !plan_flat( net.model, net.device, net.n, segs, target, net.opts, first, span, pack ) ) return false;
 	net.flat = true;
 	net.pack = pack;
 	net.flat_tmax = ( span + 31 ) / 32 * 32;
@@ -1014,7 +1055,7 @@ bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int tar
 // buffers + pivots; edges must be filled before build_pivots is enqueued
 void allocate_buffers( spk_net & net );
 
-void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs, int tile_target = 0 )
+void allocate( spk_net & net, long long n, long long width, std::vector<cost_segment> const & segs )
 {
 	require( n > 0 && n <= INT_MAX, "invalid neuron count" );
 	require( width >= 0 && width % 32 == 0, "width must be a multiple of 32" );
@@ -1027,8 +1068,8 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	net.tc = plastic_of( net.model ) ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
 	spk::model_traits const md = describe( net.model );
 
-	// window kernel and tiling: window_flat with work-balanced tiles (SPK_TILES=uniform keeps
-	// equal tiles, SPK_KERNEL=direct selects window_counts)
+	// window kernel and tiling: window_flat with work-balanced tiles (opts.uniform keeps
+	// equal tiles, opts.direct selects window_counts)
 	net.seg_start.clear();
 	net.seg_cost.clear();
 	for( auto const & g : segs )
@@ -1037,8 +1078,8 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 		net.seg_cost.push_back( g.cost );
 	}
 	net.flat = false;
-	char const * kern = getenv( "SPK_KERNEL" );
-	if( !plastic_of( net.model ) && !( kern && !strcmp( kern, "direct" ) ) ) flat_tiling( net, segs, tile_target > 0 ? tile_target : dev_sms );
+	int const target = net.opts.tile_target;
+	if( !plastic_of( net.model ) && !net.opts.direct ) flat_tiling( net, segs, target > 0 ? target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.ring_slots = 2 * net.delay;
 	allocate_buffers( net );
@@ -1114,21 +1155,22 @@ void summaries_from_ring( spk_net & net )
 	CK( cudaGetLastError() );
 }
 
-// Fixed slots (window_slots) instead of variable slices: for 10-bit nets with delay >= 4
-// whose longest slice fits 8 vectors, when the slots are at least half full on average
-// (`vectors` = the variable slices' vectors) and a step's arrivals fit the shared memory.
-// SPK_SLOTS=0 keeps the variable slices, SPK_SLOTS=1 takes slots whenever they fit.
-bool plan_slots( spk_net & net, unsigned long long vectors )
+// Fixed slots (window_slots) instead of variable slices, on request only (a checkpoint of
+// a slotted net, SPK_SLOTS=1): for 10-bit nets with delay >= 7 whose longest slice fits 8
+// vectors and whose step's arrivals fit the shared memory. On the 1e9-synapse Brunel net
+// (slots of 8 vectors) a step takes 6.47 us against window_flat's 6.22 us, so the
+// variable slices stay the default.
+bool plan_slots( spk_net & net )
 {
 	net.slot_vecs = 0;
 	net.tin = 0;
 	net.slot_data.reset();
 	net.tile_in.reset();
 	net.summ.reset();
-	char const * env = getenv( "SPK_SLOTS" );
-	bool const off = env && !strcmp( env, "0" ), force = env && !strcmp( env, "1" );
+	int const want = net.opts.slots; // 0: none; 1: where they fit; else exactly this many vectors
 	int const nt = net.tc.ntiles;
-	if( off || net.pack != 12 || net.delay < 4 || net.width == 0 ) return false;
+	require( want <= 1 || net.pack == 12, "checkpoint slots do not fit this device" );
+	if( want == 0 || net.pack != 12 || net.delay < 7 || net.width == 0 ) return false;
 	std::vector<int> in( nt ), idx( nt, -1 );
 	CK( cudaMemcpyAsync( in.data(), net.tile_inputs.p, (size_t)nt * 4, cudaMemcpyDeviceToHost, net.stream ) );
 	sbuf mx( 4, net.stream, net.device );
@@ -1144,10 +1186,10 @@ bool plan_slots( spk_net & net, unsigned long long vectors )
 	int S = 2;
 	while( S < 8 && (unsigned)S * 12 < longest ) S *= 2;
 	if( tin == 0 || (unsigned)S * 12 < longest ) return false;
-	double const full = (double)vectors / ( (double)net.n * tin * S );
 	spk::slot_geom const g = spk::slot_layout( net.classes(), net.neuron_attrs(), net.flat_tmax, nt, S, net.slot_smem );
-	if( g.ecap < spk::SLOT_MIN_ECAP || (size_t)2 * g.ecap * S * 16 < spk::slot_direct_scratch( nt ) ) return false;
-	if( !force && full < 0.5 ) return false;
+	bool const fits = g.ecap >= spk::SLOT_MIN_ECAP && spk::slot_layout_end( g, S ) <= (size_t)net.slot_smem;
+	require( want <= 1 || ( fits && S == want ), "checkpoint slots do not fit this device" );
+	if( !fits ) return false;
 	net.slot_vecs = S;
 	net.tin = tin;
 	net.tile_in.alloc( (size_t)nt * 4, net.mem() );
@@ -1185,11 +1227,10 @@ void build_slices( spk_net & net )
 		all += rv[s];
 	}
 	require( all < ( 1ULL << 32 ), "graph too large for 32-bit slice records" );
-	char const * sync = getenv( "SPK_FLAT_SYNC" );
-	net.flat_sync = sync && !strcmp( sync, "1" );
+	net.flat_sync = net.opts.flat_sync;
 	net.done_step.alloc( (size_t)nt * sizeof( long long ), net.mem() );
 	CK( cudaMemsetAsync( net.done_step.p, 0xFF, net.done_step.bytes, net.stream ) ); // -1: nothing published
-	if( plan_slots( net, all ) )
+	if( plan_slots( net ) )
 	{
 		net.slice_rec.reset();
 		net.slices.reset();
@@ -1281,7 +1322,7 @@ void validate_edges( int32_t const * edges, uint64_t n, uint64_t width )
 // of allocate, build_slices and the plastic state; slices bounded by one 16-byte vector per
 // 8 or 12 synapses plus one per non-empty (source, tile) pair, at 5 % above the expected
 // synapse count), each buffer rounded up to the allocator's 2 MiB granule.
-size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int device, int tile_target )
+size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int device, build_opts const & o )
 {
 	long long const n = (long long)l.size(), w = (long long)l.max_degree();
 	double syn = 0;
@@ -1298,8 +1339,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	{
 		std::vector<int> first;
 		int span = 0;
-		char const * kern = getenv( "SPK_KERNEL" );
-		if( !( kern && !strcmp( kern, "direct" ) ) && plan_flat( model, device, n, layout_costs( l ), tile_target > 0 ? tile_target : sms, first, span, pack ) )
+		if( !o.direct && plan_flat( model, device, n, layout_costs( l ), o.tile_target > 0 ? o.tile_target : sms, o, first, span, pack ) )
 		{
 			flat = true;
 			T = (long long)first.size() - 1;
@@ -1326,11 +1366,11 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	{
 		b.push_back( (double)n * T * 8 );
 		b.push_back( 16.0 * ( std::ceil( syn / pack ) + std::min( (double)n * T, syn ) ) );
-		if( pack == 12 && delay >= 4 )
+		if( o.slots && pack == 12 && delay >= 7 )
 		{
-			// fixed slots, taken when at least half full: at most twice the slices' vectors
-			// (built beside the slice records), and the spike-summary ring
-			b.push_back( 16.0 * ( std::ceil( syn / pack ) + std::min( (double)n * T, syn ) ) );
+			// fixed slots (on request): at most 8 vectors per (source, tile) pair, built
+			// beside the slice records, and the spike-summary ring
+			b.push_back( 128.0 * n * T );
 			b.push_back( 2.0 * delay * T * spk::SUM_W * 4 );
 			b.push_back( (double)T * 4 );
 		}
@@ -1370,7 +1410,7 @@ struct ckpt_header
 	float dt;
 	uint64_t seed, steps;
 	int32_t ntiles, flat, pack, ring_slots, flat_tmax, threads, npt, tile;
-	int32_t nbufs, reserved;
+	int32_t nbufs, slot_vecs; // window_slots' vectors per slot (0: variable slices)
 };
 constexpr char CKPT_MAGIC[8] = { 'S', 'P', 'K', 'C', 'K', 'P', 'T', '1' };
 
@@ -1458,6 +1498,8 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 				}
 		}
 	}
+	require( h.slot_vecs == 0 || ( h.flat && h.pack == 12 && h.delay >= 7 && ( h.slot_vecs == 2 || h.slot_vecs == 4 || h.slot_vecs == 8 ) ),
+	         "checkpoint tiling does not fit its kernel: slots" );
 	// the kernel shape
 	if( h.flat )
 	{
@@ -1539,6 +1581,7 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	auto net = std::make_unique<spk_net>();
 	net->model = model;
 	net->device = device;
+	net->opts = resolve_opts( nullptr ); // the automatic choices (creators with options replace them)
 	net->dt = dt;
 	net->delay = delay;
 	net->seed = seed;
@@ -1762,17 +1805,18 @@ int create_net(
     uint64_t seed,
     uint64_t graph_seed,
     int device,
-    int tile_target,
+    spk_net_options const * opts,
     bool pooled )
 {
 	return guarded( [&] {
 		require( out != nullptr, "out is null" );
-		require( tile_target >= 0, "tile target must be >= 0" );
 		*out = nullptr;
+		build_opts const o = resolve_opts( opts );
 		auto const l = to_layout( desc );
 		std::unique_ptr<spk_net> net( new_net( model, dt, delay, seed, device, pooled ) );
+		net->opts = o;
 		device_guard g( device );
-		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ), tile_target );
+		allocate( *net, (long long)l.size(), (long long)l.max_degree(), layout_costs( l ) );
 		enqueue_generate( net->stream, l, graph_seed, net->edges.as<int>(), net->conns_dev, net->mem() );
 		enqueue_pivots( *net );
 		init_state( *net );
@@ -1810,7 +1854,11 @@ int spk_net_raise_device_error( spk_net * net )
 int spk_net_create_pooled(
     spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target )
 {
-	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, tile_target, true );
+	if( tile_target < 0 ) return guarded( [] { require( false, "tile target must be >= 0" ); } );
+	spk_net_options o;
+	spk_net_options_init( &o );
+	o.tile_target = tile_target;
+	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, &o, true );
 }
 
 // Maps up to `bytes` (at most the device's free memory less 1 GiB) into the device's
@@ -1901,18 +1949,44 @@ int spk_net_create( spk_net ** out, int model, spk_layout_desc const * desc, flo
 int spk_net_create_ex(
     spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, int tile_target )
 {
-	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, tile_target, false );
+	if( tile_target < 0 ) return guarded( [] { require( false, "tile target must be >= 0" ); } );
+	spk_net_options o;
+	spk_net_options_init( &o );
+	o.tile_target = tile_target;
+	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, &o, false );
+}
+
+int spk_net_create_opts(
+    spk_net ** out, int model, spk_layout_desc const * desc, float dt, int delay, uint64_t seed, uint64_t graph_seed, int device, spk_net_options const * opts )
+{
+	return create_net( out, model, desc, dt, delay, seed, graph_seed, device, opts, false );
+}
+
+void spk_net_options_init( spk_net_options * o )
+{
+	if( !o ) return;
+	o->tile_target = 0;
+	o->kernel = o->slice_bits = o->tiling = o->persistent = o->pipelined = o->slots = -1;
+}
+
+int spk_net_estimate_bytes_opts( int model, spk_layout_desc const * desc, int delay, int device, spk_net_options const * opts, uint64_t * out_bytes )
+{
+	return guarded( [&] {
+		require( out_bytes != nullptr, "out is null" );
+		require( delay >= 1, "invalid delay" );
+		describe( model );
+		auto const l = to_layout( desc );
+		*out_bytes = estimate_bytes( model, l, delay, device, resolve_opts( opts ) );
+	} );
 }
 
 int spk_net_estimate_bytes( int model, spk_layout_desc const * desc, int delay, int device, int tile_target, uint64_t * out_bytes )
 {
-	return guarded( [&] {
-		require( out_bytes != nullptr, "out is null" );
-		require( delay >= 1 && tile_target >= 0, "invalid delay or tile target" );
-		describe( model );
-		auto const l = to_layout( desc );
-		*out_bytes = estimate_bytes( model, l, delay, device, tile_target );
-	} );
+	if( tile_target < 0 ) return guarded( [] { require( false, "invalid delay or tile target" ); } );
+	spk_net_options o;
+	spk_net_options_init( &o );
+	o.tile_target = tile_target;
+	return spk_net_estimate_bytes_opts( model, desc, delay, device, &o, out_bytes );
 }
 
 int spk_net_create_from_adj(
@@ -2201,6 +2275,7 @@ int spk_net_checkpoint( spk_net * net, void * buf, uint64_t cap, uint64_t * out_
 		h.npt = net->tc.npt;
 		h.tile = net->tc.tile;
 		h.nbufs = (int32_t)( bufs.size() + pl.size() );
+		h.slot_vecs = net->slot_vecs;
 		unsigned char * o = static_cast<unsigned char *>( buf );
 		std::memcpy( o, &h, sizeof h );
 		o += sizeof h;
@@ -2265,6 +2340,7 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		net->pack = h.pack;
 		net->flat_tmax = h.flat_tmax;
 		net->tc = { h.threads, h.npt, h.tile, h.ntiles };
+		net->opts.slots = h.slot_vecs; // the saved net's kernel and layout
 		set_tiles( *net, first );
 		net->ring_slots = h.ring_slots;
 		allocate_buffers( *net );

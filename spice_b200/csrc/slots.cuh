@@ -11,22 +11,27 @@
 // gone, and a slot of 128 bytes is one aligned line. Rows stay source-major: the tiles'
 // slots of one row are one contiguous stretch, fetched from DRAM once.
 //
-// Spike summaries. Besides the ring of spike ids, every tile publishes per step one
-// 128-byte record { count, first 31 ids } (the `summ` ring). A tile reads a step's
-// records of all source tiles in one burst of aligned lines instead of per-source-tile
-// counts and then ids.
+// Spike summaries. Besides the ring of spike ids, every tile writes per step one 128-byte
+// record { count, first 31 ids } (the `summ` ring). A tile reads the first 16 bytes of
+// every source tile's record of a step (count and three ids: all of a tile of 511
+// receiving neurons in almost every step) and, a step later, the rest of the records of
+// the few tiles that fired more, instead of per-source-tile counts and then every id.
 //
 // Pipeline (tiles with inputs). While the consumer warps count step k, the producer warps
-//   - load the summary records of step k + 2 and lay out its arrivals (a scan of the
-//     counts, then every source tile's ids into the step's entry list),
-//   - copy the slots of step k + 1's arrivals into half (k + 1) & 1 of the slot ring and,
-//     once they landed, list the vectors that hold indices (from each slot's length),
-// and the publisher warp compacts step k - 1 into the spike ring and its summary, fences
-// and publishes it, then checks the publication of step k + 3 for the producers' next
-// loads. A step with more arrivals than a ring half, or a source tile with more than 31
-// spikes, takes the direct path of window_counts (ELL rows) alone; the pipeline restarts
-// after it. Persistent runs need delay >= 4: every wait then targets a step before the
-// waiting tile's own.
+//   - load the record heads of step k + 3 and the rest of step k + 2's records, then lay
+//     out step k + 2's arrivals (a place per source tile from one shared atomic, then its
+//     ids: the order of a step's arrivals does not change its integer counts),
+//   - copy the slots of step k + 1's arrivals into the slot ring, right after step k's,
+// and the publisher warp compacts step k - 1 into the spike ring and its record, publishing
+// it (fence, then the tile's flag) every P = min(4, delay - 5) steps, and, when the records
+// the producers load next are not yet known to be published, waits for several steps at
+// once. The consumers count every slot with up to S threads, each slot's length (in its
+// first vector) telling which vectors hold indices. A step whose arrivals and the previous
+// step's do not fit the ring together, or a source tile with more than 31 spikes, runs
+// alone: its ids from the spike ring, its slots in pieces of a whole ring; the pipeline
+// restarts after it. Persistent runs need delay >= 6 (the nets use it from delay 7): every
+// wait then targets a step that every tile at the waiting tile's step or later has
+// published.
 #pragma once
 
 #include "flat.cuh"
@@ -45,9 +50,8 @@ __host__ __device__ __forceinline__ unsigned slot_len( uint4 v )
 }
 
 // Shared-memory layout of a window_slots CTA with inputs, after the fixed part of
-// window_flat (state, fired bits, counters): summaries [2][ntiles][SUM_W], their scanned
-// offsets [ntiles + 1], entry lists [2][ecap] (source ids), vector lists [2][ecap * S]
-// (16-bit ring vector indices) and the slot ring [2][ecap][S] vectors.
+// window_flat (state, fired bits, counters): summaries [2][ntiles][SUM_W], spare
+// [ntiles + 1], entry lists [2][2 ecap] (source ids) and the slot ring [2 ecap][S] vectors.
 struct slot_geom
 {
 	size_t sum, soff, ent, vl, ring;
@@ -62,24 +66,20 @@ __host__ __device__ inline slot_geom slot_layout( int classes, int attrs, int sp
 	b += (size_t)2 * ntiles * SUM_W * 4;
 	g.soff = b;
 	b += ( ( (size_t)ntiles + 1 ) * 4 + 15 ) & ~(size_t)15;
-	long long const per = 2LL * 4 + 2LL * S * 2 + 2LL * S * 16; // bytes per arrival of capacity
+	long long const per = 4LL * 4 + 2LL * S * 16; // bytes per arrival of capacity
 	long long const room = (long long)smem_bytes - (long long)b - 64;
 	int ecap = room > 0 ? (int)( room / per ) : 0;
 	ecap = ecap > SLOT_MAX_ECAP ? SLOT_MAX_ECAP : ecap & ~7;
 	g.ecap = ecap;
 	g.ent = b;
-	b += (size_t)2 * ecap * 4;
+	b += (size_t)2 * ( 2 * ecap ) * 4; // two lists of 2 ecap ids
+	b = ( b + 15 ) & ~(size_t)15;
 	g.vl = b;
-	b += ( (size_t)2 * ecap * S * 2 + 15 ) & ~(size_t)15;
 	g.ring = b;
 	return g;
 }
-
-// the direct path's scratch (per-source-tile prefix, staged arrivals) lives in the ring
-__host__ __device__ inline size_t slot_direct_scratch( int ntiles )
-{
-	return ( ( ( (size_t)ntiles + 1 ) * 4 + 15 ) & ~(size_t)15 ) + (size_t)SPIKE_BATCH * 16;
-}
+// the end of a window_slots CTA's shared memory (the slot ring's end)
+__host__ __device__ inline size_t slot_layout_end( slot_geom const & g, int S ) { return g.ring + (size_t)2 * g.ecap * S * 16; }
 
 // ------------------------------------------------------------------------------------
 // building the slots (once per net)
@@ -157,10 +157,11 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 	__shared__ long long s_t0;
 	__shared__ float s_c, s_sum;
 	// per step s (index s & 7): arrivals, too large for the pipeline; per ring half: vectors
-	__shared__ int m_e[8], m_big[8];
-	__shared__ int vcnt[2];
-	__shared__ int wsum[32];
-	__shared__ int s_big;
+	__shared__ long long s_known; // latest step every tile has published (the publisher's cache)
+	// per parity of a step: its arrivals and vectors (counted with shared atomics: the order
+	// of a step's arrivals does not change its integer counts), a source tile with more ids
+	// than its record holds
+	__shared__ int ecnt[4], eover[4], rbase[4], bigf[4];
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
 	int const nwc = nw - SLOT_PRODUCERS, ncons = nwc * 32;
@@ -176,9 +177,7 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 	unsigned * cnt = bits2 + 2 * words;
 	slot_geom const g = slot_layout( C, (int)N::size, span, p.ntiles, S, smem_bytes );
 	int * sum = reinterpret_cast<int *>( smem + g.sum );                      // [2][ntiles][SUM_W]
-	int * soff = reinterpret_cast<int *>( smem + g.soff );                    // [ntiles + 1]
-	int * ent = reinterpret_cast<int *>( smem + g.ent );                      // [2][ecap]
-	unsigned short * vl = reinterpret_cast<unsigned short *>( smem + g.vl ); // [2][ecap * S]
+	int * ent = reinterpret_cast<int *>( smem + g.ent );                      // [2][2 ecap]
 	uint4 * const ring = reinterpret_cast<uint4 *>( smem + g.ring );          // [2][ecap][S]
 	int const ecap = g.ecap;
 
@@ -249,7 +248,7 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 			if( lane == 0 ) bits[base >> 5] = word;
 		}
 	};
-	auto compact = [&]( int k ) { compact_step( p, bits2 + ( k & 1 ) * words, words, d0, tile, t0 + k, lane ); };
+	auto compact = [&]( int k, bool publish = true ) { compact_step( p, bits2 + ( k & 1 ) * words, words, d0, tile, t0 + k, lane, publish ); };
 
 	if( !inputs )
 	{
@@ -270,6 +269,29 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 	}
 	else
 	{
+		// every index of the E slots from ring slot `b0` on (wrapping around the ring of R
+		// slots), T threads per slot (T a power of two: as many as the threads allow, at most
+		// S): a slot's length (its first vector) tells how many vectors hold indices
+		auto count_slots = [&]( int b0, int E, int t, int nthr ) {
+			if( E <= 0 ) return;
+			int lt = 0;
+			while( ( 1 << lt ) < S && ( 2 << lt ) * E <= nthr ) lt++;
+			int const T = 1 << lt, RR = 2 * ecap;
+#pragma unroll 1
+			for( int x = t; x < E * T; x += nthr )
+			{
+				int const e = x >> lt, h = x & ( T - 1 );
+				int r = b0 + e;
+				if( r >= RR ) r -= RR;
+				uint4 const * sl = ring + (size_t)r * S;
+				int const nv = min( S, (int)( slot_len( sl[0] ) + 11 ) / 12 );
+				for( int v = h; v < nv; v += T ) count_vector<12>( cnt, sl[v] );
+			}
+		};
+		// publication every P steps (each publication covers the steps before it)
+		int const P = min( 4, p.delay - 5 );
+		auto compact_lazy = [&]( int k ) { compact( k, ( ( t0 + k ) % P ) == P - 1 || k == L - 1 ); };
+		int const R = 2 * ecap; // the slot ring: consecutive steps' arrivals follow each other
 		int k = 0;
 		while( k < L )
 		{
@@ -277,43 +299,63 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 			// producer work during step j (the prologue: j < kb, every thread): threads
 			// [0, npt) of numbering pt; `all` when every warp of the CTA takes part
 			auto produce = [&]( int j, int pt, int npt, bool all ) {
-				int const sa = j + 2, sb = j + 1;
-				bool const do_s = sa >= kb && sa < L;
-				bool const do_a = sb >= kb && sb < L && !m_big[sb & 7];
+				int const s3 = j + 3, sa = j + 2, sb = j + 1;
+				bool const do_sa = sa >= kb && sa < L;
+				// step sb's place in the ring: after step j's arrivals (none before kb); too
+				// many arrivals for the ring, or more ids than a record holds: the step runs alone
+				int const eb = ecnt[sb & 3];
+				int const prev = sb > kb ? ecnt[j & 3] : 0;
+				int const base = sb > kb ? ( rbase[j & 3] + prev ) % R : 0;
+				bool const big = eover[sb & 3] || eb + prev > R;
+				bool const do_a = sb >= kb && sb < L && !big;
 				if( pt == 0 )
 				{
-					vcnt[sb & 1] = 0;
-					s_big = 0;
+					bigf[sb & 3] = big;
+					rbase[sb & 3] = base;
+					ecnt[sa & 3] = 0;
+					eover[sa & 3] = 0;
 				}
-				// summaries of step sa (none before `delay`): eight lanes per source tile; in
-				// the prologue every lane first waits for the step's publication (later steps:
-				// checked by the publisher warp during the step before)
-				if( do_s )
+				// the first 16 bytes (count, three ids) of every summary record of step s3 (none
+				// before `delay`); in the prologue every thread first waits for the step's
+				// publication (later steps: checked by the publisher warp ahead of time)
+				if( s3 >= kb && s3 < L )
 				{
-					long long const t = t0 + sa;
-					int * sd = sum + ( sa & 1 ) * p.ntiles * SUM_W;
+					long long const t = t0 + s3;
+					int * sd = sum + ( s3 & 1 ) * p.ntiles * SUM_W;
 					if( t >= p.delay )
 					{
 						int const * src = p.summ + ( ( t - p.delay ) % p.ring ) * (long long)p.ntiles * SUM_W;
-						int const q = pt & 7;
-						for( int i = pt >> 3; i < p.ntiles; i += npt >> 3 )
+						for( int i = pt; i < p.ntiles; i += npt )
 						{
 							if( all ) wait_published( p, i, t - p.delay );
-							cp_async16( sd + i * SUM_W + 4 * q, src + i * SUM_W + 4 * q );
+							cp_async16( sd + i * SUM_W, src + i * SUM_W );
 						}
 					}
 					else
 						for( int i = pt; i < p.ntiles; i += npt ) sd[i * SUM_W] = 0;
 				}
-				// slots of step sb's arrivals into ring half sb & 1: S lanes per arrival
+				// the rest of the records of step sa whose tile fired more than three neurons
+				if( do_sa && t0 + sa >= p.delay )
+				{
+					int * sd = sum + ( sa & 1 ) * p.ntiles * SUM_W;
+					int const * src = p.summ + ( ( t0 + sa - p.delay ) % p.ring ) * (long long)p.ntiles * SUM_W;
+					for( int i = pt; i < p.ntiles; i += npt )
+					{
+						int const need = min( SUM_W, sd[i * SUM_W] + 1 ); // ints of the record in use
+						for( int v = 4; v < need; v += 4 ) cp_async16( sd + i * SUM_W + v, src + i * SUM_W + v );
+					}
+				}
+				// the slots of step sb's arrivals, S lanes per arrival
 				if( do_a )
 				{
-					int const E = m_e[sb & 7];
-					int const * es = ent + ( sb & 1 ) * ecap;
-					uint4 * rh = ring + (size_t)( sb & 1 ) * ecap * S;
+					int const * es = ent + ( sb & 1 ) * ecap * 2;
 					int const q = pt % S, groups = npt / S;
-					for( int e = pt / S; e < E; e += groups )
-						cp_async16( rh + e * S + q, p.slots + ( (long long)es[e] * p.tin + ti ) * S + q );
+					for( int e = pt / S; e < eb; e += groups )
+					{
+						int r = base + e;
+						if( r >= R ) r -= R;
+						cp_async16( ring + (size_t)r * S + q, p.slots + ( (long long)es[e] * p.tin + ti ) * S + q );
+					}
 				}
 				cp_async_commit();
 				cp_async_wait_all();
@@ -321,137 +363,127 @@ __device__ __forceinline__ void window_slots_body( net_params const & p, int con
 					__syncthreads();
 				else
 					bar_sync_slot_producers();
-				// the vectors of step sb that hold indices, from every slot's length
-				if( do_a )
-				{
-					int const E = m_e[sb & 7];
-					uint4 const * rh = ring + (size_t)( sb & 1 ) * ecap * S;
-					unsigned short * vo = vl + ( sb & 1 ) * ecap * S;
-					int const rbase = ( sb & 1 ) * ecap * S;
-					for( int e0 = pt - lane; e0 < E; e0 += npt )
-					{
-						int const e = e0 + lane;
-						int nv = 0;
-						if( e < E ) nv = min( S, (int)( slot_len( rh[e * S] ) + 11 ) / 12 );
-						int const incl = warp_inclusive_scan( nv );
-						int base = 0;
-						if( lane == 31 && incl ) base = atomicAdd( &vcnt[sb & 1], incl );
-						base = __shfl_sync( 0xffffffffu, base, 31 );
-						int const o = base + incl - nv;
-						for( int v = 0; v < nv; v++ ) vo[o + v] = (unsigned short)( rbase + e * S + v );
-					}
-				}
-				// step sa: counts -> offsets of its arrivals (a scan over the source tiles),
-				// then every source tile's ids into the entry list
-				if( do_s )
+				// step sa's arrivals: a place in its entry list per source tile from one shared
+				// atomic (the order of a step's arrivals does not change its integer counts),
+				// then the tile's ids
+				if( do_sa )
 				{
 					int const * sd = sum + ( sa & 1 ) * p.ntiles * SUM_W;
-					int const nwp = npt >> 5, pw = pt >> 5;
-					int run = 0;
-					for( int i0 = 0; i0 < p.ntiles; i0 += npt )
+					int * es = ent + ( sa & 1 ) * ecap * 2;
+					for( int i = pt; i < p.ntiles; i += npt )
 					{
-						int const i = i0 + pt;
-						int const c = i < p.ntiles ? sd[i * SUM_W] : 0;
-						if( c > SUM_W - 1 ) s_big = 1; // more ids than the record holds
-						int const incl = warp_inclusive_scan( c );
-						if( lane == 31 ) wsum[pw] = incl;
-						if( all )
-							__syncthreads();
-						else
-							bar_sync_slot_producers();
-						int before = run;
-						for( int w = 0; w < pw; w++ ) before += wsum[w];
-						if( i < p.ntiles ) soff[i] = before + incl - c;
-						for( int w = 0; w < nwp; w++ ) run += wsum[w];
-						if( all )
-							__syncthreads();
-						else
-							bar_sync_slot_producers();
-					}
-					bool const big = s_big != 0; // set before the scan's barriers
-					if( pt == 0 )
-					{
-						soff[p.ntiles] = run;
-						m_e[sa & 7] = run;
-						m_big[sa & 7] = big || run > ecap;
-					}
-					if( !big && run <= ecap )
-					{
-						int * es = ent + ( sa & 1 ) * ecap;
-						for( int i = pt; i < p.ntiles; i += npt )
-						{
-							int const c = sd[i * SUM_W], o = soff[i];
-							for( int r = 0; r < c; r++ ) es[o + r] = sd[i * SUM_W + 1 + r];
-						}
+						int const c = sd[i * SUM_W];
+						if( c == 0 ) continue;
+						if( c > SUM_W - 1 ) eover[sa & 3] = 1; // more ids than the record holds
+						int const o = atomicAdd( &ecnt[sa & 3], c );
+						int const cc = min( c, SUM_W - 1 );
+						for( int r = 0; r < cc && o + r < R; r++ ) es[o + r] = sd[i * SUM_W + 1 + r];
 					}
 				}
 			};
 
-			int ks = L; // a step for the direct path, if any
+			int ks = L; // a step for the synchronous path, if any
 			if( !p.flat_sync )
 			{
-				for( int j = kb - 2; j < kb; j++ )
+				for( int j = kb - 3; j < kb; j++ )
 				{
 					produce( j, tid, nt, true );
 					__syncthreads();
 				}
 				// the publication of the step whose summaries the producers load during step
-				// kb (later ones: checked by the publisher warp a step ahead)
-				if( kb + 2 < L && t0 + kb + 2 >= p.delay )
-					for( int i = tid; i < p.ntiles; i += nt ) wait_published( p, i, t0 + kb + 2 - p.delay );
+				// kb (later ones: checked by the publisher warp ahead of time)
+				if( kb + 3 < L && t0 + kb + 3 >= p.delay )
+					for( int i = tid; i < p.ntiles; i += nt ) wait_published( p, i, t0 + kb + 3 - p.delay );
+				if( tid == 0 ) s_known = t0 + kb + 3 - p.delay;
 				__syncthreads();
 				for( ; k < L; k++ )
 				{
-					if( m_big[k & 7] )
+					if( bigf[k & 3] )
 					{
-						ks = k;
+						ks = k; // this step takes the synchronous path
 						break;
 					}
 					advance_clock( k );
 					if( warp < nwc )
 					{
-						if( t0 + k >= p.delay )
-						{
-							int const v = vcnt[k & 1];
-							unsigned short const * vo = vl + ( k & 1 ) * ecap * S;
-#pragma unroll 2
-							for( int x = tid; x < v; x += ncons ) count_vector<12>( cnt, ring[vo[x]] );
-						}
+						if( t0 + k >= p.delay ) count_slots( rbase[k & 3], ecnt[k & 3], tid, ncons );
 						bar_sync_first( ncons ); // counts complete
 						update( k, nwc );
 					}
 					else if( warp == nw - 1 )
 					{
-						// the publisher warp: step k - 1's spikes and summary, fenced, then its
-						// flag; then the publication of the step whose summaries the producers
-						// load during the next step
-						if( k > kb ) compact( k - 1 );
-						if( k + 3 < L && t0 + k + 3 >= p.delay ) warp_wait_all_published( p, t0 + k + 3 - p.delay );
+						// the publisher warp: step k - 1's spikes and summary (published every P
+						// steps, fenced); then, when the summaries the producers load next step
+						// are not known to be published, a wait for several steps at once
+						if( k > kb ) compact_lazy( k - 1 );
+						long long const need = t0 + k + 4 - p.delay;
+						if( k + 4 < L && need >= 0 && need > s_known )
+						{
+							long long const demand = min( t0 + k - P - 1, need + 7 );
+							warp_wait_all_published( p, demand );
+							if( lane == 0 ) s_known = demand;
+						}
 					}
 					else
 						produce( k, tid - ncons, nt - ncons - 32, false );
 					__syncthreads(); // step k updated, step k + 1's slots in the ring
 				}
-				if( k > kb && warp == nw - 1 ) compact( k - 1 ); // the last pipelined step
+				if( k > kb && warp == nw - 1 ) compact( k - 1 ); // the last pipelined step, published
 				__syncthreads();
 			}
 			else
 				ks = k;
 			if( ks >= L ) break;
 
-			// ------------------------------------------------------------ the direct path
-			// step ks alone from the ELL rows (window_counts' path), its scratch in the ring
+			// ------------------------------------------------------------ the synchronous path
+			// step ks alone: its arrivals' ids from the spike ring, their slots in pieces of up
+			// to a whole ring (both halves), each counted before the next is copied
 			advance_clock( ks );
 			long long const t = t0 + ks;
 			if( t >= p.delay )
 			{
-				int * pref = reinterpret_cast<int *>( ring );
-				int4 * sbuf = reinterpret_cast<int4 *>( reinterpret_cast<unsigned char *>( ring ) + ( ( ( p.ntiles + 1 ) * 4 + 15 ) & ~15 ) );
-				net_params q = p;
-				q.tile = span; // counter rows are span long
+				int const slot_in = (int)( ( t - p.delay ) % p.ring );
+				int * pref = sum; // [ntiles + 1] per-source-tile prefix of the step's spikes
 				for( int i = tid; i < p.ntiles; i += nt ) wait_published( p, i, t - p.delay );
 				__syncthreads();
-				deliver_counts<N>( q, (int)( ( t - p.delay ) % p.ring ), tile, d0, d1, cnt, pref, sbuf, scratch );
+				int running = 0;
+				for( int base = 0; base < p.ntiles; base += nt )
+				{
+					int const i = base + tid;
+					int const c = i < p.ntiles ? (int)p.ring_cnt[(long long)slot_in * p.ntiles + i] : 0;
+					int tot;
+					int const ex = block_exclusive_scan( c, scratch, &tot );
+					if( i < p.ntiles ) pref[i] = running + ex;
+					running += tot;
+				}
+				if( tid == 0 ) pref[p.ntiles] = running;
+				__syncthreads();
+				int const M = running, R = 2 * ecap;
+				for( int b0 = 0; b0 < M; b0 += R )
+				{
+					int const m = min( R, M - b0 );
+					for( int x = tid; x < m; x += nt )
+					{
+						int const g = b0 + x;
+						int lo = 0, hi = p.ntiles; // largest i with pref[i] <= g
+						while( hi - lo > 1 )
+						{
+							int const mid = ( lo + hi ) >> 1;
+							if( pref[mid] <= g )
+								lo = mid;
+							else
+								hi = mid;
+						}
+						int const src = p.ring_ids[(long long)slot_in * p.n + __ldg( p.tile_first + lo ) + ( g - pref[lo] )];
+						uint4 const * from = p.slots + ( (long long)src * p.tin + ti ) * S;
+						for( int v = 0; v < S; v++ ) cp_async16( ring + (size_t)x * S + v, from + v );
+					}
+					cp_async_commit();
+					cp_async_wait_all();
+					__syncthreads();
+					count_slots( 0, m, tid, nt );
+					__syncthreads();
+				}
 			}
 			__syncthreads();
 			update( ks, nw );

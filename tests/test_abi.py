@@ -61,6 +61,34 @@ def test_layout_matches_reference_known_answers(lib):
     assert L([70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)]).max_degree() == 7328
 
 
+def test_net_options_checked_without_device(lib):
+    """Build choices (spk_net_options): automatic by default, checked before device work."""
+    import ctypes as C
+
+    o = spice_b200.net_options()
+    assert o.tile_target == 0
+    assert [getattr(o, f) for f in ("kernel", "slice_bits", "tiling", "persistent", "pipelined", "slots")] == [-1] * 6
+    o = spice_b200.net_options(7, kernel="direct", slice_bits=16, tiling="uniform", persistent=False, pipelined=False, slots=True)
+    assert (o.tile_target, o.kernel, o.slice_bits, o.tiling, o.persistent, o.pipelined, o.slots) == (7, 1, 16, 1, 0, 0, 1)
+    with pytest.raises(spice_b200.InvalidArgument):
+        spice_b200.net_options(colour="red")
+    with pytest.raises(spice_b200.InvalidArgument):
+        spice_b200.net_options(slice_bits=12)
+    with pytest.raises(spice_b200.InvalidArgument):
+        spice_b200.net_options(-1)
+    d = spice_b200.Layout([100, 100], [(0, 1, 0.1)]).desc()
+    h = C.c_void_p()
+    bad = spice_b200.net_options()
+    bad.slice_bits = 12
+    assert lib.spk_net_create_opts(C.byref(h), 0, C.byref(d), 1e-4, 1, 1, 1, 0, C.byref(bad)) == spice_b200.ERR_INVALID
+    assert b"slice_bits" in lib.spk_last_error()
+    bad = spice_b200.net_options()
+    bad.tile_target = -3
+    out = C.c_uint64()
+    assert lib.spk_net_estimate_bytes_opts(0, C.byref(d), 1, 0, C.byref(bad), C.byref(out)) == spice_b200.ERR_INVALID
+    assert lib.spk_net_estimate_bytes(0, C.byref(d), 1, 0, -3, C.byref(out)) == spice_b200.ERR_INVALID
+
+
 def test_server_and_batch_arguments_checked_without_device(lib):
     import ctypes as C
 

@@ -365,19 +365,10 @@ def test_flat_kernel_matches_direct_kernel(n, delay, steps, stage, deg):
     itself checked against the oracle above, on nets too large for the oracle to step
     quickly."""
     layout = Layout(n, deg / n)
-    env = {"sync": ("SPK_FLAT_SYNC", "1"), "uniform": ("SPK_TILES", "uniform")}
-    for f in (stage.split("+") if stage else []):
-        os.environ[env[f][0]] = env[f][1]
-    try:
-        a = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
-    finally:
-        for k, _ in env.values():
-            os.environ.pop(k, None)
-    os.environ["SPK_KERNEL"] = "direct"
-    try:
-        b = Snn("synth", layout, delay=delay, seed=3, graph_seed=9)
-    finally:
-        del os.environ["SPK_KERNEL"]
+    choice = {"sync": ("pipelined", False), "uniform": ("tiling", "uniform")}
+    opts = dict(choice[f] for f in (stage.split("+") if stage else []))
+    a = Snn("synth", layout, delay=delay, seed=3, graph_seed=9, options=opts)
+    b = Snn("synth", layout, delay=delay, seed=3, graph_seed=9, options={"kernel": "direct"})
     ca, ia = a.run_record(steps, cap=n * steps // 50)
     cb, ib = b.run_record(steps, cap=n * steps // 50)
     assert ca.max() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
@@ -399,11 +390,7 @@ def test_persistent_run_matches_windows(model, pops, conns, delay, steps):
     spikes, against the same steps as windowed launches (checked against the oracle above)."""
     layout = Layout(pops, conns)
     a = Snn(model, layout, delay=delay, seed=5, graph_seed=11)
-    os.environ["SPK_PERSIST"] = "0"
-    try:
-        b = Snn(model, layout, delay=delay, seed=5, graph_seed=11)
-    finally:
-        del os.environ["SPK_PERSIST"]
+    b = Snn(model, layout, delay=delay, seed=5, graph_seed=11, options={"persistent": False})
     a.run(steps)
     b.run(steps)
     for x, y in zip(a.neurons(), b.neurons()):
@@ -490,13 +477,12 @@ def test_batch_rejects_stepped_retile_and_double_add():
 
 
 @pytest.mark.parametrize("model,kernel", [("brunel_with_plasticity", None), ("brunel", "direct")])
-def test_nets_of_one_model_with_different_shared_memory(model, kernel, monkeypatch):
+def test_nets_of_one_model_with_different_shared_memory(model, kernel):
     """A kernel's shared-memory limit is shared by all nets: a smaller net created after a
     larger one must not break the larger one's launches."""
-    if kernel:
-        monkeypatch.setenv("SPK_KERNEL", kernel)
-    big = Snn(model, Layout([20_000, 20_000], [(0, 1, 0.02), (1, 1, 0.02)]), delay=15)
-    small = Snn(model, Layout([300, 300], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15)
+    opts = {"kernel": kernel} if kernel else None
+    big = Snn(model, Layout([20_000, 20_000], [(0, 1, 0.02), (1, 1, 0.02)]), delay=15, options=opts)
+    small = Snn(model, Layout([300, 300], [(0, 1, 0.1), (1, 1, 0.1)]), delay=15, options=opts)
     big.run(30)
     small.run(30)
     big.sync()
@@ -512,11 +498,7 @@ def test_recording_runs_equal_windowed_recording(n, delay, chunks):
     spike ring) against run_record over windows; runs and stepped output after it agree."""
     layout = Layout([n // 2, n // 2], [(0, 1, 16 / n), (1, 1, 16 / n)])
     a = Snn("synth" if delay == 6 else "brunel", layout, delay=delay, seed=8, graph_seed=8)
-    os.environ["SPK_PERSIST"] = "0"
-    try:
-        b = Snn("synth" if delay == 6 else "brunel", layout, delay=delay, seed=8, graph_seed=8)
-    finally:
-        del os.environ["SPK_PERSIST"]
+    b = Snn("synth" if delay == 6 else "brunel", layout, delay=delay, seed=8, graph_seed=8, options={"persistent": False})
     assert a.info().persistent == 1 and b.info().persistent == 0
     a.run(37)
     b.run(37)
@@ -537,12 +519,11 @@ def test_recording_runs_equal_windowed_recording(n, delay, chunks):
     ("vogels_abbott", [30_000], [(0, 0, 0.02)], 8),
     ("synth", [150_000], [(0, 0, 16 / 150_000)], 4),
 ])
-def test_ten_bit_slices_match_sixteen_bit(model, pops, conns, delay, monkeypatch):
+def test_ten_bit_slices_match_sixteen_bit(model, pops, conns, delay):
     """Slices packed twelve 10-bit indices to a vector against eight 16-bit ones."""
     layout = Layout(pops, conns)
     a = Snn(model, layout, delay=delay, seed=6, graph_seed=6)
-    monkeypatch.setenv("SPK_PACK", "16")
-    b = Snn(model, layout, delay=delay, seed=6, graph_seed=6)
+    b = Snn(model, layout, delay=delay, seed=6, graph_seed=6, options={"slice_bits": 16})
     assert a.info().slice_pack == 12 and b.info().slice_pack == 8
     ca, ia = a.run_record(300, cap=sum(pops) * 300 // 4)
     cb, ib = b.run_record(300, cap=sum(pops) * 300 // 4)
@@ -736,20 +717,19 @@ def test_withheld_publication_ends_the_launch_with_a_timeout(monkeypatch):
 SLOT_NETS = [
     ("brunel", [20_000, 20_000], [(0, 1, 0.05), (1, 1, 0.05)], 15, 600),   # the pipeline, persistent
     ("vogels_abbott", [30_000], [(0, 0, 0.02)], 8, 400),
-    ("synth", [150_000], [(0, 0, 16 / 150_000)], 4, 300),                 # delay 4: the shortest look-ahead
-    ("synth", [150_000], [(0, 0, 0.01)], 6, 100),                         # 750 arrivals a step, slots of 2 vectors
+    ("synth", [150_000], [(0, 0, 16 / 150_000)], 7, 300),                 # delay 7: the shortest look-ahead
+    ("synth", [150_000], [(0, 0, 0.01)], 8, 100),                         # 750 arrivals a step, slots of 2 vectors
     ("brunel", [60_000, 4_000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 200),    # Poisson tiles of > 31 spikes: direct steps
 ]
 
 
 @pytest.mark.parametrize("model,pops,conns,delay,steps", SLOT_NETS)
-def test_slots_match_variable_slices(model, pops, conns, delay, steps, monkeypatch):
-    """window_slots (fixed slots, spike summaries) against window_flat (variable slices) on
-    the same net: persistent recording runs, then windowed steps, bit for bit."""
+def test_slots_match_variable_slices(model, pops, conns, delay, steps):
+    """window_slots (fixed slots, spike summaries) against window_flat (variable slices, the
+    automatic choice) on the same net: persistent recording runs, then windowed steps, bit
+    for bit."""
     layout = Layout(pops, conns)
-    monkeypatch.setenv("SPK_SLOTS", "1")
-    a = Snn(model, layout, delay=delay, seed=3, graph_seed=9)
-    monkeypatch.setenv("SPK_SLOTS", "0")
+    a = Snn(model, layout, delay=delay, seed=3, graph_seed=9, options={"slots": True})
     b = Snn(model, layout, delay=delay, seed=3, graph_seed=9)
     assert a.info().slot_vecs > 0 and b.info().slot_vecs == 0
     ca, ia = a.run_record(steps, cap=sum(pops) * steps // 4)
@@ -766,7 +746,8 @@ def test_slots_match_variable_slices(model, pops, conns, delay, steps, monkeypat
 
 
 def test_slots_against_the_oracle(monkeypatch):
-    """A slotted Brunel net against the oracle, spike by spike, and its persistent run."""
+    """A slotted Brunel net against the oracle, spike by spike, and its persistent run (the
+    slots chosen by the SPK_SLOTS test override of the automatic choice)."""
     monkeypatch.setenv("SPK_SLOTS", "1")
     net, ref = run_parity("brunel", [3000, 3000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 700, 4, graph_seed=14)
     assert net.info().slot_vecs > 0
@@ -781,16 +762,15 @@ def test_slotted_nets_in_a_batch_and_restored(monkeypatch):
     """window_slots_batch (slotted nets in shared launches, beside nets with variable
     slices) and a slotted net's checkpoint (its summaries rebuilt from the spike ring)."""
     nets = [("brunel", [10_000, 10_000], [(0, 1, 0.1), (1, 1, 0.1)], 15), ("vogels_abbott", [20_000], [(0, 0, 0.02)], 8),
-            ("synth", [100_000], [(0, 0, 30 / 100_000)], 6)]
+            ("synth", [100_000], [(0, 0, 30 / 100_000)], 9)]
     batch = spice_b200.Batch()
     alone, batched = [], []
     for i, (model, pops, conns, delay) in enumerate(nets):
-        for slots in ("1", "0"):
-            monkeypatch.setenv("SPK_SLOTS", slots)
-            a = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7)
-            b = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7)
-            b.set_tile_target(24 + 10 * i)
-            assert (b.info().slot_vecs > 0) == (slots == "1")
+        for slots in (True, False):
+            a = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7, options={"slots": slots})
+            b = Snn(model, Layout(pops, conns), delay=delay, seed=i + 1, graph_seed=i + 7, options={"slots": slots})
+            b.set_tile_target((40, 60, 110)[i])  # enough tiles for 10-bit slices
+            assert (b.info().slot_vecs > 0) == slots
             batch.add(b)
             alone.append(a)
             batched.append(b)
@@ -807,8 +787,9 @@ def test_slotted_nets_in_a_batch_and_restored(monkeypatch):
     s = alone[0]
     assert s.info().slot_vecs > 0
     s.run_record(300, cap=20_000 * 300)  # an enlarged ring
+    monkeypatch.setenv("SPK_SLOTS", "0")  # the checkpoint's layout wins
     r = Snn.restore(s.checkpoint())
-    assert r.info().slot_vecs > 0
+    assert r.info().slot_vecs == s.info().slot_vecs
     ca, ia = s.run_record(100, cap=20_000 * 100)
     cb, ib = r.run_record(100, cap=20_000 * 100)
     assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
