@@ -38,7 +38,11 @@ typedef enum spk_model
 	   counterpart; see each header): */
 	SPK_VOGELS_ABBOTT_NS = 4, /* include/spice/models/vogels_abbott_ns.h: 0.27 / 4.5 nS, V uniform in [-60, -50) mV */
 	SPK_BRUNEL_FIXED = 5,     /* include/spice/models/brunel_fixed.h: reset 10 mV, J = 0.1 / -0.5 mV */
-	SPK_BRUNEL_PLUS_A012 = 6  /* include/spice/models/brunel_with_plasticity_a012.h: A- = 0.012 */
+	SPK_BRUNEL_PLUS_A012 = 6, /* include/spice/models/brunel_with_plasticity_a012.h: A- = 0.012 */
+	/* a model of the user's, compiled into a build of the library with
+	   -DSPK_USER_MODEL_HEADER='"header.h"' -DSPK_USER_MODEL=its::type (spice_b200.build.build_user);
+	   absent (SPK_ERR_INVALID) from the default build */
+	SPK_USER_MODEL_ID = 7
 } spk_model;
 
 /* Population sizes and (src_pop, dst_pop, p) connection list: the arguments of
@@ -149,7 +153,10 @@ int spk_net_create_ex(
 typedef struct spk_net_options
 {
     int tile_target; /* window_flat tiles: about this many; 0 = one per SM */
-    int kernel;      /* SPK_KERNEL: 0 = window kernels (window_flat where the model allows), 1 = per-step kernels ("direct") */
+    int kernel;      /* SPK_KERNEL: 0 = window kernels (window_flat where the model allows), 1 = window_counts ("direct"),
+                        2 = window_ordered ("ordered": the generic kernel, every arrival through the model's receive()
+                        in the reference CPU simulator's order; the only kernel of models without input classes or with
+                        synapse attributes, and of no plastic model) */
     int slice_bits;  /* SPK_PACK: 10 = 10-bit target indices where every index fits (12 to a vector), 16 = 16-bit (8 to a vector) */
     int tiling;      /* SPK_TILES: 0 = tiles balanced by per-neuron cost, 1 = equal tiles ("uniform") */
     int persistent;  /* SPK_PERSIST: 1 = one cooperative launch per run when every tile's CTA is resident, 0 = windowed launches */

@@ -19,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "libspice_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libspice_ref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libspice_ref_fast.so")
+# the reference's cpu::snn of the tests' model (tests/user_model), as model 7
+REF_USER_LIB = os.path.join(HERE, "_ref", "libspice_ref_user.so")
 # the reference checkout the `ref` build compiles from (no default: set by the build recipe)
 REFERENCE_SRC = os.environ.get("SPICE_REFERENCE_SRC", "")
 
@@ -206,8 +208,8 @@ class OracleNet:
 _rlibs = {}
 
 
-def ref_lib(fast=False):
-    path = REF_FAST_LIB if fast else REF_LIB
+def ref_lib(fast=False, path=None):
+    path = path or (REF_FAST_LIB if fast else REF_LIB)
     if path not in _rlibs:
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path}: the reference build is not available")
@@ -237,23 +239,28 @@ def ref_lib(fast=False):
 class ReferenceNet:
     """The reference's cpu::snn (with the counter-RNG Poisson stream)."""
 
-    def __init__(self, model, pops, conns, dt=1e-4, delay=1, seed=1, fast=False, _state=None):
-        lib = ref_lib(fast)
+    def __init__(self, model, pops, conns, dt=1e-4, delay=1, seed=1, fast=False, _state=None, lib_path=None,
+                 types=None):
+        lib = ref_lib(fast, lib_path)
         self.lib = lib
         self.model = MODELS[model] if isinstance(model, str) else int(model)
+        # attribute dtypes (neuron, synapse): the built-in models' unless given
+        if types is None:
+            types = (NEURON_ATTRS[self.model], [np.float32] * 3 if self.model in PLASTIC else [])
+        self.neuron_types, self.synapse_types = list(types[0]), list(types[1])
         if _state is None:
             self._h = lib.ref_create(self.model, *_layout_args(pops, conns), dt, delay, seed)
         else:
             edges, width, neurons, synapses, step0, counts, ids = _state
             e = np.ascontiguousarray(edges, dtype=np.int32)
             n = e.size // width if width else len(neurons[0])
-            na = [np.ascontiguousarray(a, dtype=t) for a, t in zip(neurons, NEURON_ATTRS[self.model])]
-            sa = [np.ascontiguousarray(a, dtype=np.float32) for a in synapses] if synapses else []
+            na = [np.ascontiguousarray(a, dtype=t) for a, t in zip(neurons, self.neuron_types)]
+            sa = [np.ascontiguousarray(a, dtype=t) for a, t in zip(synapses, self.synapse_types)] if synapses else []
             c = np.ascontiguousarray(counts, dtype=np.uint32)
             i = np.ascontiguousarray(ids, dtype=np.int32)
             self._h = lib.ref_create_from_state(self.model, n, width, e.ctypes.data_as(IP),
                                                 (C.c_void_p * len(na))(*[a.ctypes.data for a in na]),
-                                                (C.c_void_p * 3)(*[a.ctypes.data for a in sa]) if sa else None,
+                                                (C.c_void_p * len(sa))(*[a.ctypes.data for a in sa]) if sa else None,
                                                 dt, delay, seed, int(step0), len(c), c.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                 i.ctypes.data_as(IP))
         if not self._h:
@@ -264,14 +271,14 @@ class ReferenceNet:
 
     @classmethod
     def from_state(cls, model, edges, width, neurons, synapses=None, dt=1e-4, delay=1, seed=1, fast=False, step0=0,
-                   counts=(), ids=()):
+                   counts=(), ids=(), lib_path=None, types=None):
         """The reference's cpu::snn over a given graph (n x width ELL) and state (neuron
         attribute arrays; for Brunel+ also W, Zpre, Zpost over all slots): a simulation that
         continues where another one stands at step `step0` (clock and Poisson stream keyed by
         `seed`), with the spikes of the last len(counts) steps in flight (counts per step, ids
         concatenated, oldest first)."""
         return cls(model, None, None, dt=dt, delay=delay, seed=seed, fast=fast,
-                   _state=(edges, int(width), neurons, synapses, step0, counts, ids))
+                   _state=(edges, int(width), neurons, synapses, step0, counts, ids), lib_path=lib_path, types=types)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -288,13 +295,13 @@ class ReferenceNet:
         return e[: self.n * self.width], self.width
 
     def neurons(self):
-        arrs = [np.empty(self.n, dtype=t) for t in NEURON_ATTRS[self.model]]
+        arrs = [np.empty(self.n, dtype=t) for t in self.neuron_types]
         self.lib.ref_neurons(self._h, (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs]))
         return arrs
 
     def synapses(self):
-        if self.model not in PLASTIC:
+        if not self.synapse_types:
             return []
-        arrs = [np.empty(self.n * self.width, dtype=np.float32) for _ in range(3)]
-        self.lib.ref_synapses(self._h, (C.c_void_p * 3)(*[a.ctypes.data for a in arrs]))
+        arrs = [np.empty(self.n * self.width, dtype=t) for t in self.synapse_types]
+        self.lib.ref_synapses(self._h, (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs]))
         return arrs

@@ -12,6 +12,18 @@
 #include <spice/util/adj_list.h>
 #include <spice/util/layout.h>
 
+// A model of the tests compiled in as model 7 (the `user` target of oracle/Makefile): the
+// reference's snn and cpu::snn definitions are included here, instead of linking snn.cpp and
+// snn.h.cpp, so that both can be instantiated for it.
+#if defined( SPK_USER_MODEL_HEADER ) && defined( SPK_USER_MODEL )
+#include <spice/cpu/snn.h.cpp>
+#include <spice/snn.cpp>
+#include SPK_USER_MODEL_HEADER
+template class spice::snn<SPK_USER_MODEL>;
+template class spice::cpu::snn<SPK_USER_MODEL>;
+#define SPK_HAS_USER_MODEL 1
+#endif
+
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -110,6 +122,9 @@ SPICE_HARNESS_ACCESS( spice::vogels_abbott )
 SPICE_HARNESS_ACCESS( spice::brunel )
 SPICE_HARNESS_ACCESS( spice::brunel_with_plasticity )
 SPICE_HARNESS_ACCESS( spice::synth )
+#if defined( SPK_HAS_USER_MODEL )
+SPICE_HARNESS_ACCESS( SPK_USER_MODEL )
+#endif
 #undef SPICE_HARNESS_ACCESS
 
 template <typename Tuple, size_t... I>
@@ -356,6 +371,9 @@ void * ref_create_from_state(
 		case 1: return make( std::common_type<spice::brunel>{} );
 		case 2: return make( std::common_type<spice::brunel_with_plasticity>{} );
 		case 3: return make( std::common_type<spice::synth>{} );
+#if defined( SPK_HAS_USER_MODEL )
+		case 7: return make( std::common_type<SPK_USER_MODEL>{} );
+#endif
 		default: g_err = "invalid model"; return nullptr;
 		}
 	}

@@ -19,11 +19,15 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libspice_b200.so")
+# SPICE_B200_LIB selects another build of the library: one with a model of the user's
+# compiled in (spice_b200.build.build_user), reached as model "user"
+LIB_PATH = os.environ.get("SPICE_B200_LIB") or os.path.join(_HERE, "libspice_b200.so")
 
 MODELS = {"vogels_abbott": 0, "brunel": 1, "brunel_with_plasticity": 2, "synth": 3,
           # the benchmark configurations' constants (include/spice/models/*.h)
-          "vogels_abbott_ns": 4, "brunel_fixed": 5, "brunel_with_plasticity_a012": 6}
+          "vogels_abbott_ns": 4, "brunel_fixed": 5, "brunel_with_plasticity_a012": 6,
+          # SPK_USER_MODEL_ID: present in user builds only
+          "user": 7}
 MODEL_NAMES = {v: k for k, v in MODELS.items()}
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_DEVICE, ERR_CAPACITY, ERR_TIMEOUT = range(7)
@@ -103,7 +107,7 @@ class _NetOptions(C.Structure):
 
 # build choices (spk_net_options): name -> (field, {value: int})
 _OPTION_VALUES = {
-    "kernel": {"window": 0, "direct": 1},
+    "kernel": {"window": 0, "direct": 1, "ordered": 2},
     "slice_bits": {10: 10, 16: 16},
     "tiling": {"balanced": 0, "uniform": 1},
     "persistent": {False: 0, True: 1},
@@ -113,7 +117,7 @@ _OPTION_VALUES = {
 
 
 def net_options(tile_target=0, **choices):
-    """spk_net_options from keyword choices (kernel="window"|"direct", slice_bits=10|16,
+    """spk_net_options from keyword choices (kernel="window"|"direct"|"ordered", slice_bits=10|16,
     tiling="balanced"|"uniform", persistent=bool, pipelined=bool, slots=bool); a choice
     left out is automatic."""
     o = _NetOptions()

@@ -2,6 +2,11 @@
 
     python -m spice_b200.build            # builds spice_b200/libspice_b200.so
 
+A model of the user's is compiled in beside the library's own models by build_user(header,
+type, out): the same sources with -DSPK_USER_MODEL_HEADER / -DSPK_USER_MODEL, the model
+reachable as C-ABI id SPK_USER_MODEL_ID (7). Models are template arguments of the kernels,
+as in the reference (spice/cuda/snn.d.cpp:247-250), so a new model means a new build.
+
 Flags that matter:
   -gencode arch=compute_100a,code=sm_100a   B200 only
   -fmad=false     no contraction of a*b+c into fma: the models' arithmetic stays
@@ -17,7 +22,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspice_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "net.cu"), os.path.join(HERE, "csrc", "server.cpp")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "plastic.cuh", "flat.cuh", "device_common.cuh")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in
+                  ("kernels.cuh", "plastic.cuh", "flat.cuh", "slots.cuh", "ordered.cuh", "models.cuh", "device_common.cuh")]
+USER_MODEL_ID = 7
 
 
 def nvcc_path():
@@ -42,6 +49,26 @@ def command(out=LIB, extra=()):
         "-lcudart",
         *extra,
     ]
+
+
+def build_user(header, model, out, force=False, verbose=False):
+    """libspice_b200 with the model `model` (a C++ type name) of `header` compiled in as model
+    id USER_MODEL_ID; written to `out`. Rebuilt when a source, header or the model header is
+    newer than `out`."""
+    header = os.path.abspath(header)
+    if not force and os.path.exists(out):
+        t = os.path.getmtime(out)
+        if all(os.path.getmtime(f) <= t for f in DEPS + _headers() + [header]):
+            return out
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    cmd = command(out=out, extra=[f'-DSPK_USER_MODEL_HEADER="{header}"', f"-DSPK_USER_MODEL={model}",
+                                  "-I", os.path.dirname(header)])
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    return out
 
 
 def _headers():

@@ -59,6 +59,7 @@ struct net_params
 	unsigned const * pivots;
 	int const * tile_first; // [ntiles + 1] first neuron of every tile
 	void * attr[MAX_ATTRS];
+	void * syn_attr[MAX_ATTRS]; // static synapse attribute k, [n x width] parallel to edges (window_ordered)
 	int * ring_ids;
 	unsigned * ring_cnt;
 	clock_state * clock;
@@ -234,6 +235,39 @@ __device__ __forceinline__ void window_clock_end( net_params const & p, int L, l
 			__threadfence();
 		}
 	}
+}
+
+// The exclusive prefix over the source tiles' entry counts of ring slot `slot` (pref[0..ntiles]),
+// and the slot's total.
+__device__ __forceinline__ int stage_prefix( net_params const & p, unsigned const * cnt_ring, int slot, int * pref, int * scratch )
+{
+	int running = 0;
+	for( int base = 0; base < p.ntiles; base += blockDim.x )
+	{
+		int const i = base + threadIdx.x;
+		int const c = i < p.ntiles ? (int)cnt_ring[(long long)slot * p.ntiles + i] : 0;
+		int tot;
+		int const ex = block_exclusive_scan( c, scratch, &tot );
+		if( i < p.ntiles ) pref[i] = running + ex;
+		running += tot;
+	}
+	if( threadIdx.x == 0 ) pref[p.ntiles] = running;
+	__syncthreads();
+	return running;
+}
+
+__device__ __forceinline__ int find_tile( int const * pref, int ntiles, int g )
+{
+	int lo = 0, hi = ntiles;
+	while( hi - lo > 1 )
+	{
+		int const mid = ( lo + hi ) >> 1;
+		if( pref[mid] <= g )
+			lo = mid;
+		else
+			hi = mid;
+	}
+	return lo;
 }
 
 // ------------------------------------------------------------------------------------

@@ -13,6 +13,14 @@
 #include <spice/models/vogels_abbott_ns.h>
 #include <spice_b200.h>
 
+// a model compiled in beside the library's own (a user build, the tests' model): the
+// header that defines it (SPK_USER_MODEL_HEADER) and its type (SPK_USER_MODEL), C-ABI id
+// SPK_USER_MODEL_ID
+#if defined( SPK_USER_MODEL_HEADER ) && defined( SPK_USER_MODEL )
+#include SPK_USER_MODEL_HEADER
+#define SPK_HAS_USER_MODEL 1
+#endif
+
 #include <type_traits>
 
 namespace spk
@@ -23,7 +31,11 @@ struct model_tag
 	using type = M;
 };
 
-constexpr int MODEL_COUNT = 7;
+#if defined( SPK_HAS_USER_MODEL )
+constexpr int MODEL_COUNT = SPK_USER_MODEL_ID + 1;
+#else
+constexpr int MODEL_COUNT = SPK_USER_MODEL_ID;
+#endif
 
 // f(model_tag<Model>{}) for the model with C-ABI id `model`; false if there is none
 template <typename F>
@@ -38,20 +50,28 @@ bool with_model( int model, F && f )
 	case SPK_VOGELS_ABBOTT_NS: f( model_tag<spice::vogels_abbott_ns>{} ); return true;
 	case SPK_BRUNEL_FIXED: f( model_tag<spice::brunel_fixed>{} ); return true;
 	case SPK_BRUNEL_PLUS_A012: f( model_tag<spice::brunel_with_plasticity_a012>{} ); return true;
+#if defined( SPK_HAS_USER_MODEL )
+	case SPK_USER_MODEL_ID: f( model_tag<SPK_USER_MODEL>{} ); return true;
+#endif
 	default: return false;
 	}
 }
 
 template <typename Model>
 constexpr bool is_plastic_model = Model::synapse::has_stdp;
-// models the window_flat kernels run: input classes, no plasticity
+// models the counting kernels (window_flat, window_slots, window_counts) run: input classes,
+// no plasticity, no synapse attributes (the counts replay knows only the source's class)
 template <typename Model>
-constexpr bool is_flat_model = Model::neuron::input_classes > 0 && !Model::synapse::has_stdp;
+constexpr bool is_flat_model = Model::neuron::input_classes > 0 && !Model::synapse::has_stdp && Model::synapse::size == 0;
+// models that only the generic kernel (window_ordered) runs: the other non-plastic ones
+template <typename Model>
+constexpr bool needs_ordered = !Model::synapse::has_stdp && !is_flat_model<Model>;
 
 struct model_traits
 {
 	bool plastic;
-	int classes;       // input classes (0 for plastic models)
+	bool ordered;      // runs on window_ordered only (needs_ordered)
+	int classes;       // input classes (0 for plastic models and the models window_ordered runs)
 	int neuron_attrs;
 	int synapse_attrs; // as exported (the reference's synapse tuple)
 	char types[16];    // 'f' / 'i' per neuron attribute, then per exported synapse attribute
@@ -75,11 +95,13 @@ model_traits traits_of()
 	using E = typename Model::synapse::export_tuple_t;
 	model_traits t{};
 	t.plastic = is_plastic_model<Model>;
-	t.classes = t.plastic ? 0 : N::input_classes;
+	t.ordered = needs_ordered<Model>;
+	t.classes = is_flat_model<Model> ? N::input_classes : 0;
 	t.neuron_attrs = (int)N::size;
-	t.synapse_attrs = t.plastic ? (int)std::tuple_size<E>::value : 0;
+	t.synapse_attrs = (int)std::tuple_size<E>::value;
+	static_assert( N::size + std::tuple_size<E>::value < sizeof( model_traits::types ), "too many attributes" );
 	tuple_chars<typename N::tuple_t>( t.types, std::make_index_sequence<N::size>() );
-	if( t.plastic ) tuple_chars<E>( t.types + t.neuron_attrs, std::make_index_sequence<std::tuple_size<E>::value>() );
+	tuple_chars<E>( t.types + t.neuron_attrs, std::make_index_sequence<std::tuple_size<E>::value>() );
 	return t;
 }
 } // namespace spk

@@ -7,6 +7,7 @@
 #include "kernels.cuh"
 #include "flat.cuh"
 #include "models.cuh"
+#include "ordered.cuh"
 #include "plastic.cuh"
 #include "slots.cuh"
 
@@ -313,6 +314,7 @@ spk::model_traits describe( int model )
 }
 
 bool plastic_of( int model ) { return describe( model ).plastic; }
+bool ordered_of( int model ) { return describe( model ).ordered; }
 int classes_of( int model ) { return describe( model ).classes; }
 int neuron_attrs_of( int model ) { return describe( model ).neuron_attrs; }
 
@@ -390,6 +392,7 @@ struct build_opts
 {
 	int tile_target = 0;   // 0: one tile per SM
 	bool direct = false;   // per-step kernels instead of the window kernels
+	bool ordered = false;  // the generic window_ordered kernel for any non-plastic model
 	bool pack16 = false;   // 16-bit slice indices even where 10-bit ones fit
 	bool uniform = false;  // equal tiles instead of cost-balanced ones
 	bool windowed = false; // no persistent launch
@@ -417,7 +420,11 @@ build_opts resolve_opts( spk_net_options const * o )
 	require( d.slice_bits == -1 || d.slice_bits == 10 || d.slice_bits == 16, "slice_bits must be 10 or 16" );
 	build_opts r;
 	r.tile_target = d.tile_target;
-	r.direct = pick( d.kernel, "SPK_KERNEL", "direct", "window", false );
+	require( d.kernel >= -1 && d.kernel <= 2, "kernel must be 0 (window), 1 (direct) or 2 (ordered)" );
+	char const * ke = getenv( "SPK_KERNEL" );
+	int const kernel = d.kernel >= 0 ? d.kernel : !ke ? 0 : !strcmp( ke, "direct" ) ? 1 : !strcmp( ke, "ordered" ) ? 2 : 0;
+	r.direct = kernel == 1;
+	r.ordered = kernel == 2;
 	r.pack16 = d.slice_bits >= 0 ? d.slice_bits == 16 : env_is( "SPK_PACK", "16" );
 	r.uniform = pick( d.tiling, "SPK_TILES", "uniform", "balanced", false );
 	r.windowed = !pick( d.persistent, "SPK_PERSIST", "1", "0", true );
@@ -461,6 +468,8 @@ struct spk_net
 	dbuf edges, pivots, tile_first, ring_ids, ring_cnt, clock, dt_ring, err, conns_dev;
 	std::vector<int> tile_first_host; // [ntiles + 1]
 	dbuf attr[spk::MAX_ATTRS];
+	dbuf syn[spk::MAX_ATTRS]; // static synapse attributes (window_ordered models), [n x width] each
+	bool ordered = false;     // window_ordered: every arrival through the model's receive(), in order
 	dbuf gather_ids, gather_cnt, cursor, gather_done, rec_ids, rec_cnt;
 	spk::plastic_state plast; // plastic models only
 
@@ -519,6 +528,7 @@ struct spk_net
 		p.pivots = pivots.as<unsigned const>();
 		p.tile_first = tile_first.as<int const>();
 		for( int i = 0; i < spk::MAX_ATTRS; i++ ) p.attr[i] = attr[i].p;
+		for( int i = 0; i < spk::MAX_ATTRS; i++ ) p.syn_attr[i] = syn[i].p;
 		p.ring_ids = ring_ids.as<int>();
 		p.ring_cnt = ring_cnt.as<unsigned>();
 		p.clock = clock.as<spk::clock_state>();
@@ -547,6 +557,7 @@ struct spk_net
 		           rec_cnt.bytes + plast.bytes() + slices.bytes + slice_rec.bytes + tile_inputs.bytes + done_step.bytes +
 		           slot_data.bytes + tile_in.bytes + summ.bytes;
 		for( auto const & a : attr ) b += a.bytes;
+		for( auto const & a : syn ) b += a.bytes;
 		return b;
 	}
 
@@ -560,6 +571,7 @@ struct spk_net
 		size_t const head = ( (size_t)classes * tc.tile + tc.ntiles + 1 ) * 4;
 		size_t b = ( ( head + 15 ) & ~(size_t)15 ) + (size_t)spk::SPIKE_BATCH * 16;
 		if( plastic_of( model ) ) b = spk::plastic_window_smem( tc.tile, tc.ntiles, tc.threads );
+		if( ordered ) b = spk::ordered_window_smem( tc.tile, tc.ntiles );
 		return (int)b;
 	}
 
@@ -579,12 +591,19 @@ struct spk_net
 		}
 		else
 		{
-			switch( tc.npt )
-			{
-			case 4: f( spk::window_counts<Model, 4> ); break;
-			case 2: f( spk::window_counts<Model, 2> ); break;
-			default: f( spk::window_counts<Model, 1> ); break;
-			}
+			if( ordered )
+				switch( tc.npt )
+				{
+				case 2: f( spk::window_ordered<Model, 2> ); break;
+				default: f( spk::window_ordered<Model, 1> ); break;
+				}
+			else if constexpr( spk::is_flat_model<Model> )
+				switch( tc.npt )
+				{
+				case 4: f( spk::window_counts<Model, 4> ); break;
+				case 2: f( spk::window_counts<Model, 2> ); break;
+				default: f( spk::window_counts<Model, 1> ); break;
+				}
 		}
 	}
 
@@ -592,7 +611,7 @@ struct spk_net
 	void configure_model()
 	{
 		int const smem = window_smem();
-		if constexpr( Model::neuron::input_classes > 0 )
+		if constexpr( spk::is_flat_model<Model> )
 			if( flat )
 			{
 				// all the shared memory a CTA can have: what the fixed parts leave over
@@ -654,12 +673,16 @@ struct spk_net
 			auto const q = plast.params();
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, q, L, dt ); } );
 		}
-		else if( flat && slot_vecs )
-		{
-			if constexpr( spk::is_flat_model<Model> ) spk::window_slots<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
-		}
 		else if( flat )
-			spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+		{
+			if constexpr( spk::is_flat_model<Model> )
+			{
+				if( slot_vecs )
+					spk::window_slots<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+				else
+					spk::window_flat<Model><<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt, smem );
+			}
+		}
 		else
 			with_window_kernel<Model>( [&]( auto kernel ) { kernel<<<tc.ntiles, tc.threads, smem, stream>>>( p, L, dt ); } );
 		CK( cudaGetLastError() );
@@ -777,7 +800,7 @@ struct spk_net
 	template <typename Model>
 	void launch_persistent_model( int L )
 	{
-		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
+		if constexpr( spk::is_flat_model<Model> )
 		{
 			auto p = params();
 			// window_flat's step pipeline looks five steps ahead, which needs delay >= 6;
@@ -842,6 +865,12 @@ void init_model( spk_net & net )
 	spk::init_neurons<Model><<<std::max( 1, blocks ), 256, 0, net.stream>>>( p );
 	CK( cudaGetLastError() );
 	if constexpr( Model::synapse::has_stdp ) spk::init_plastic<Model>( p, net.plast, net.dt, net.sms, net.stream );
+	else if constexpr( Model::synapse::size > 0 )
+		if( net.n * net.width > 0 )
+		{
+			spk::init_synapses<Model><<<4 * net.sms, 256, 0, net.stream>>>( p );
+			CK( cudaGetLastError() );
+		}
 }
 
 void init_state( spk_net & net )
@@ -1065,8 +1094,11 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	int dev_sms = 0;
 	CK( cudaDeviceGetAttribute( &dev_sms, cudaDevAttrMultiProcessorCount, net.device ) );
 	net.sms = dev_sms;
-	net.tc = plastic_of( net.model ) ? choose_tiles( n, dev_sms, 512, 1 ) : choose_tiles( n, dev_sms, 2048, 4 );
 	spk::model_traits const md = describe( net.model );
+	net.ordered = !md.plastic && ( md.ordered || net.opts.ordered );
+	net.tc = md.plastic ? choose_tiles( n, dev_sms, 512, 1 )
+	         : net.ordered ? choose_tiles( n, dev_sms, spk::ORD_MAX_TILE, 2 )
+	                       : choose_tiles( n, dev_sms, 2048, 4 );
 
 	// window kernel and tiling: window_flat with work-balanced tiles (opts.uniform keeps
 	// equal tiles, opts.direct selects window_counts)
@@ -1079,7 +1111,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	}
 	net.flat = false;
 	int const target = net.opts.tile_target;
-	if( !plastic_of( net.model ) && !net.opts.direct ) flat_tiling( net, segs, target > 0 ? target : dev_sms );
+	if( !md.plastic && !net.ordered && !net.opts.direct ) flat_tiling( net, segs, target > 0 ? target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.ring_slots = 2 * net.delay;
 	allocate_buffers( net );
@@ -1112,6 +1144,13 @@ void allocate_buffers( spk_net & net )
 	CK( cudaMemsetAsync( net.cursor.p, 0, 8, net.stream ) );
 	CK( cudaMemsetAsync( net.gather_done.p, 0, 4, net.stream ) );
 	if( plastic_of( net.model ) ) net.plast.allocate( n, width, net.tc.ntiles, net.delay, net.stream, net.pool );
+	else
+		for( int i = 0; i < md.synapse_attrs; i++ )
+		{
+			// zero on padding slots, as the reference's value-initialised synapse vector
+			net.syn[i].alloc( (size_t)( n * width ) * 4, net.mem() );
+			CK( cudaMemsetAsync( net.syn[i].p, 0, net.syn[i].bytes, net.stream ) );
+		}
 	if( !net.host_count ) net.host_count = pinned_slots::get();
 	net.configure();
 }
@@ -1119,7 +1158,7 @@ void allocate_buffers( spk_net & net )
 template <typename Model>
 void fill_slices( spk_net & net, sbuf const & bases )
 {
-	if constexpr( Model::neuron::input_classes > 0 )
+	if constexpr( spk::is_flat_model<Model> )
 	{
 		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
 		spk::slice_fill<Model><<<blocks, 256, 0, net.stream>>>(
@@ -1132,7 +1171,7 @@ void fill_slices( spk_net & net, sbuf const & bases )
 template <typename Model>
 void fill_slots( spk_net & net )
 {
-	if constexpr( Model::neuron::input_classes > 0 )
+	if constexpr( spk::is_flat_model<Model> )
 	{
 		int const blocks = (int)( ( net.n * 32 + 255 ) / 256 );
 		spk::slot_fill<Model><<<blocks, 256, 0, net.stream>>>(
@@ -1331,11 +1370,14 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	syn = std::min( syn * 1.05, (double)n * w );
 	int sms = 0;
 	CK( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ) );
-	int const attrs = describe( model ).neuron_attrs;
+	spk::model_traits const md = describe( model );
+	int const attrs = md.neuron_attrs;
 	bool flat = false;
 	long long T = 0;
 	int pack = 8;
-	if( !plastic_of( model ) )
+	if( !md.plastic && ( md.ordered || o.ordered ) )
+		T = choose_tiles( n, sms, spk::ORD_MAX_TILE, 2 ).ntiles;
+	else if( !md.plastic )
 	{
 		std::vector<int> first;
 		int span = 0;
@@ -1362,6 +1404,8 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	                          4,
 	                          4096 };
 	for( int i = 0; i < attrs; i++ ) b.push_back( (double)n * 4 );
+	if( !md.plastic )
+		for( int i = 0; i < md.synapse_attrs; i++ ) b.push_back( (double)n * w * 4 );
 	if( flat )
 	{
 		b.push_back( (double)n * T * 8 );
@@ -1409,7 +1453,7 @@ struct ckpt_header
 	int32_t delay;
 	float dt;
 	uint64_t seed, steps;
-	int32_t ntiles, flat, pack, ring_slots, flat_tmax, threads, npt, tile;
+	int32_t ntiles, flat, pack, ring_slots, flat_tmax, threads, npt, tile; // flat: 1 window_flat, 2 window_ordered
 	int32_t nbufs, slot_vecs; // window_slots' vectors per slot (0: variable slices)
 };
 constexpr char CKPT_MAGIC[8] = { 'S', 'P', 'K', 'C', 'K', 'P', 'T', '1' };
@@ -1420,7 +1464,10 @@ std::vector<std::pair<uint32_t, void *>> ckpt_buffers( spk_net & net )
 	std::vector<std::pair<uint32_t, void *>> b;
 	auto add = [&]( uint32_t id, auto & buf ) { b.push_back( { id, static_cast<void *>( &buf ) } ); };
 	add( 1, net.edges );
-	for( int i = 0; i < describe( net.model ).neuron_attrs; i++ ) add( 10 + i, net.attr[i] );
+	spk::model_traits const md = describe( net.model );
+	for( int i = 0; i < md.neuron_attrs; i++ ) add( 10 + i, net.attr[i] );
+	if( !md.plastic )
+		for( int i = 0; i < md.synapse_attrs; i++ ) add( 30 + i, net.syn[i] );
 	add( 20, net.ring_ids );
 	add( 21, net.ring_cnt );
 	add( 22, net.clock );
@@ -1486,7 +1533,7 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 			if( e[k] != INT_MAX ) target[e[k]] = 1;
 		for( int j = 0; j < T; j++ )
 			for( int d = first[j]; d < first[j + 1] && !in_tile[j]; d++ ) in_tile[j] = target[d];
-		if( h.flat )
+		if( h.flat == 1 )
 		{
 			unsigned const pad = h.pack == 12 ? spk::SLICE_PAD10 : spk::SLICE_PAD;
 			for( int j = 0; j < T; j++ )
@@ -1498,10 +1545,17 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 				}
 		}
 	}
-	require( h.slot_vecs == 0 || ( h.flat && h.pack == 12 && h.delay >= 7 && ( h.slot_vecs == 2 || h.slot_vecs == 4 || h.slot_vecs == 8 ) ),
+	require( h.slot_vecs == 0 || ( h.flat == 1 && h.pack == 12 && h.delay >= 7 && ( h.slot_vecs == 2 || h.slot_vecs == 4 || h.slot_vecs == 8 ) ),
 	         "checkpoint tiling does not fit its kernel: slots" );
 	// the kernel shape
-	if( h.flat )
+	spk::model_traits const md = describe( h.model );
+	require( h.flat >= 0 && h.flat <= 2 && ( h.flat != 1 || md.classes > 0 ) && ( h.flat == 2 || !md.ordered ) && ( h.flat != 2 || !plastic ),
+	         "checkpoint kernel does not fit the model" );
+	if( h.flat == 2 )
+		require( ( h.npt == 1 || h.npt == 2 ) && h.threads >= 32 && h.threads <= 512 && h.threads % 32 == 0 && h.tile == h.threads * h.npt &&
+		             h.tile <= spk::ORD_MAX_TILE && first == uniform_tiles( h.n, h.tile ),
+		         "checkpoint tiling does not fit its kernel" );
+	else if( h.flat )
 	{
 		require( !plastic && T + 1 < spk::FLAT_PC && h.threads == spk::FLAT_THREADS && h.npt == 1 && h.tile == h.flat_tmax &&
 		             h.flat_tmax >= 32 && h.flat_tmax <= spk::FLAT_MAX_TILE && h.flat_tmax % 32 == 0,
@@ -1650,7 +1704,7 @@ struct spk_batch
 	template <typename Model>
 	static void launch_model( group & g, int4 const * jobs, int njobs, int smem, bool slotted )
 	{
-		if constexpr( Model::neuron::input_classes > 0 && !Model::synapse::has_stdp )
+		if constexpr( spk::is_flat_model<Model> )
 		{
 			if( slotted )
 				spk::window_slots_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
@@ -2036,6 +2090,9 @@ int spk_net_set_synapses( spk_net * net, void * const * attrs )
 			if constexpr( spk::is_plastic_model<M> )
 				net->plast.import<M>( net->params(), static_cast<float const *>( attrs[0] ), static_cast<float const *>( attrs[1] ),
 				                      static_cast<float const *>( attrs[2] ), net->dt, net->sms, net->stream );
+			else
+				for( int i = 0; i < md.synapse_attrs; i++ )
+					CK( cudaMemcpyAsync( net->syn[i].p, attrs[i], net->syn[i].bytes, cudaMemcpyHostToDevice, net->stream ) );
 		} );
 		CK( cudaStreamSynchronize( net->stream ) );
 	} );
@@ -2237,6 +2294,9 @@ int spk_net_synapses( spk_net * net, void * const * attrs )
 			if constexpr( spk::is_plastic_model<M> )
 				CK( net->plast.export_synapses<M>( net->params(), static_cast<float *>( attrs[0] ), static_cast<float *>( attrs[1] ),
 				                                   static_cast<float *>( attrs[2] ), net->sms, net->stream ) );
+			else
+				for( int i = 0; i < md.synapse_attrs; i++ )
+					CK( cudaMemcpyAsync( attrs[i], net->syn[i].p, net->syn[i].bytes, cudaMemcpyDeviceToHost, net->stream ) );
 		} );
 		CK( cudaStreamSynchronize( net->stream ) );
 	} );
@@ -2267,7 +2327,7 @@ int spk_net_checkpoint( spk_net * net, void * buf, uint64_t cap, uint64_t * out_
 		h.seed = net->seed;
 		h.steps = net->steps;
 		h.ntiles = net->tc.ntiles;
-		h.flat = net->flat ? 1 : 0;
+		h.flat = net->flat ? 1 : net->ordered ? 2 : 0;
 		h.pack = net->pack;
 		h.ring_slots = net->ring_slots;
 		h.flat_tmax = net->flat_tmax;
@@ -2336,7 +2396,8 @@ int spk_net_restore( spk_net ** out, void const * buf, uint64_t size, int device
 		net->n = h.n;
 		net->width = h.width;
 		CK( cudaDeviceGetAttribute( &net->sms, cudaDevAttrMultiProcessorCount, device ) );
-		net->flat = h.flat != 0;
+		net->flat = h.flat == 1;
+		net->ordered = h.flat == 2;
 		net->pack = h.pack;
 		net->flat_tmax = h.flat_tmax;
 		net->tc = { h.threads, h.npt, h.tile, h.ntiles };

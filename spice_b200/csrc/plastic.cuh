@@ -118,38 +118,6 @@ __device__ __forceinline__ float replay_post(
 	return w;
 }
 
-// Stage the entries of ring slot `slot` (prefix over the source tiles' counts).
-__device__ __forceinline__ int stage_prefix( net_params const & p, unsigned const * cnt_ring, int slot, int * pref, int * scratch )
-{
-	int running = 0;
-	for( int base = 0; base < p.ntiles; base += blockDim.x )
-	{
-		int const i = base + threadIdx.x;
-		int const c = i < p.ntiles ? (int)cnt_ring[(long long)slot * p.ntiles + i] : 0;
-		int tot;
-		int const ex = block_exclusive_scan( c, scratch, &tot );
-		if( i < p.ntiles ) pref[i] = running + ex;
-		running += tot;
-	}
-	if( threadIdx.x == 0 ) pref[p.ntiles] = running;
-	__syncthreads();
-	return running;
-}
-
-__device__ __forceinline__ int find_tile( int const * pref, int ntiles, int g )
-{
-	int lo = 0, hi = ntiles;
-	while( hi - lo > 1 )
-	{
-		int const mid = ( lo + hi ) >> 1;
-		if( pref[mid] <= g )
-			lo = mid;
-		else
-			hi = mid;
-	}
-	return lo;
-}
-
 // entries [b0, b0 + m) of the spike slot -> sb (src, slice bounds, meta)
 __device__ __forceinline__ void stage_spikes( net_params const & p, plastic_params const & q, int slot, int tile, int const * pref, int b0, int m, stage_e * sb )
 {

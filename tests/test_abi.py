@@ -189,3 +189,20 @@ def test_restore_checks_contents_before_device_work(lib):
     ids[n:n + 2] = [3, 3]  # not ascending
     rc, msg = restore(_checkpoint_bytes(edges, n, width, ring_cnt=cnt, ring_ids=ids))
     assert rc == spice_b200.ERR_INVALID and b"spike ring" in msg
+
+
+def test_user_model_build_exports_the_model():
+    """A build with the tests' model compiled in (spice_b200.build.build_user) exposes it as
+    model "user" with its attribute types; the default build rejects that id."""
+    import subprocess
+    import sys
+
+    here = os.path.join(ROOT, "tests", "user_model")
+    out = os.path.join(here, "libspice_b200_weighted_lif.so")
+    sb_build.build_user(os.path.join(here, "weighted_lif.h"), "test_models::weighted_lif", out)
+    env = dict(os.environ, SPICE_B200_LIB=out)
+    r = subprocess.run([sys.executable, os.path.join(here, "check_weighted_lif.py"), "abi"], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "abi ok" in r.stdout, r.stdout + r.stderr
+    with pytest.raises(spice_b200.InvalidArgument):
+        spice_b200.model_attrs("user")
