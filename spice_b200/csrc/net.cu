@@ -379,6 +379,19 @@ tile_cfg choose_tiles( long long n, int sms, int max_tile, int max_npt )
 		}
 	return best;
 }
+
+// Tiles of a plastic net, one neuron per thread. Every tile scans every arrival of a step,
+// so a net whose tiles of up to 512 neurons fit one per SM keeps those (one CTA per SM); a
+// larger net takes tiles of up to PL_THREADS neurons for PL_CTAS_PER_SM CTAs per SM, all
+// resident at once, instead of a second wave of CTAs. At Brunel+ 5e8 (100,000 neurons):
+// 285 tiles of 352, 0.52-0.54 wall/bio against 0.64 for the same tiles one CTA per SM
+// (two waves).
+tile_cfg plastic_tiles( long long n, int sms )
+{
+	tile_cfg const one = choose_tiles( n, sms, 512, 1 );
+	if( one.ntiles <= sms ) return one;
+	return choose_tiles( n, spk::PL_CTAS_PER_SM * sms, spk::PL_THREADS, 1 );
+}
 } // namespace
 
 namespace
@@ -582,12 +595,11 @@ struct spk_net
 	{
 		if constexpr( Model::synapse::has_stdp )
 		{
-			switch( tc.npt )
-			{
-			case 4: f( spk::window_plastic<Model, 4> ); break;
-			case 2: f( spk::window_plastic<Model, 2> ); break;
-			default: f( spk::window_plastic<Model, 1> ); break;
-			}
+			// one neuron per thread (plastic_tiles); two CTAs per SM where the tiles need it
+			if( plastic_two_per_sm() )
+				f( spk::window_plastic<Model, 1, spk::PL_CTAS_PER_SM> );
+			else
+				f( spk::window_plastic<Model, 1, 1> );
 		}
 		else
 		{
@@ -694,6 +706,9 @@ struct spk_net
 	}
 
 	int max_window() const { return std::min( delay, spk::MAX_WINDOW ); }
+
+	// window_plastic's two-CTAs-per-SM form: more tiles than SMs, each of at most PL_THREADS
+	bool plastic_two_per_sm() const { return tc.ntiles > sms && tc.threads <= spk::PL_THREADS; }
 
 	// launch every queued step
 	void flush()
@@ -1096,7 +1111,7 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	net.sms = dev_sms;
 	spk::model_traits const md = describe( net.model );
 	net.ordered = !md.plastic && ( md.ordered || net.opts.ordered );
-	net.tc = md.plastic ? choose_tiles( n, dev_sms, 512, 1 )
+	net.tc = md.plastic ? plastic_tiles( n, dev_sms )
 	         : net.ordered ? choose_tiles( n, dev_sms, spk::ORD_MAX_TILE, 2 )
 	                       : choose_tiles( n, dev_sms, 2048, 4 );
 
@@ -1390,7 +1405,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 			T = choose_tiles( n, sms, 2048, 4 ).ntiles;
 	}
 	else
-		T = choose_tiles( n, sms, 512, 1 ).ntiles;
+		T = plastic_tiles( n, sms ).ntiles;
 	std::vector<double> b = { (double)n * w * 4,
 	                          (double)n * ( T + 1 ) * 4,
 	                          2.0 * delay * n * 4,
@@ -1564,7 +1579,8 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 	else
 	{
 		require( ( h.npt == 1 || h.npt == 2 || h.npt == 4 ) && h.threads >= 32 && h.threads <= 512 && h.threads % 32 == 0 &&
-		             h.tile == h.threads * h.npt && h.tile <= ( plastic ? 512 : 2048 ) && first == uniform_tiles( h.n, h.tile ),
+		             h.tile == h.threads * h.npt && h.tile <= ( plastic ? 512 : 2048 ) && ( !plastic || h.npt == 1 ) &&
+		             first == uniform_tiles( h.n, h.tile ),
 		         "checkpoint tiling does not fit its kernel" );
 	}
 	// the spike ring: per slot and tile, an ascending run of the tile's own neurons
@@ -1636,6 +1652,7 @@ spk_net * new_net( int model, float dt, int delay, unsigned long long seed, int 
 	net->model = model;
 	net->device = device;
 	net->opts = resolve_opts( nullptr ); // the automatic choices (creators with options replace them)
+	CK( cudaDeviceGetAttribute( &net->sms, cudaDevAttrMultiProcessorCount, device ) );
 	net->dt = dt;
 	net->delay = delay;
 	net->seed = seed;
