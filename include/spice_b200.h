@@ -281,8 +281,10 @@ typedef struct spk_batch spk_batch;
 int spk_net_set_tile_target( spk_net * net, int target );
 
 int spk_batch_create( spk_batch ** out, int device );
-/* Nets of the models without plasticity (SPK_VOGELS_ABBOTT, SPK_BRUNEL, SPK_SYNTH), on the
- * batch's device; a net belongs to at most one batch. */
+/* Nets of any model, on the batch's device; a net belongs to at most one batch. The nets
+ * of one model share launches (window_flat_batch, window_slots_batch, window_plastic_batch:
+ * one CTA per (net, tile), a round of up to each net's delay in steps); nets of the generic
+ * kernel (window_ordered) and of window_counts run their own windows beside them. */
 int spk_batch_add( spk_batch * batch, spk_net * net );
 int spk_batch_remove( spk_batch * batch, spk_net * net );
 /* Advance every net of the batch by `nsteps` steps (asynchronous against the host up to

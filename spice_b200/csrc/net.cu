@@ -659,15 +659,23 @@ struct spk_net
 			}
 		// the limit is per kernel, shared by every net: set it to all a CTA can have, so a
 		// net configured later with smaller needs does not lower it under an earlier net's
-		with_window_kernel<Model>( [&]( auto kernel ) {
-			int optin = 0;
-			CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
+		int optin = 0;
+		CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
+		auto full_limit = [&]( void const * kernel ) {
 			cudaFuncAttributes fa{};
 			CK( cudaFuncGetAttributes( &fa, kernel ) );
 			int const limit = optin - (int)fa.sharedSizeBytes;
-			require( smem <= limit, "shared memory too small for the tiling" );
-			set_smem_limit( (void const *)kernel, device, limit );
-		} );
+			set_smem_limit( kernel, device, limit );
+			return limit;
+		};
+		with_window_kernel<Model>( [&]( auto kernel ) { require( smem <= full_limit( (void const *)kernel ), "shared memory too small for the tiling" ); } );
+		// a batch's shared launches of plastic nets (either form)
+		if constexpr( spk::is_plastic_model<Model> )
+		{
+			int const one = full_limit( (void const *)spk::window_plastic_batch<Model, 1> );
+			int const two = full_limit( (void const *)spk::window_plastic_batch<Model, spk::PL_CTAS_PER_SM> );
+			require( smem <= std::min( one, two ), "shared memory too small for the tiling" );
+		}
 	}
 
 	void configure()
@@ -1688,8 +1696,9 @@ struct spk_batch
 	{
 		cudaStream_t stream = nullptr;
 		cudaEvent_t ev = nullptr;
-		dbuf d_params, d_jobs;
+		dbuf d_params, d_jobs, d_pls;
 		std::vector<spk::net_params> h_params, c_params; // this run's / on the device
+		std::vector<spk::plastic_params> h_pls, c_pls;   // plastic groups
 		std::vector<int4> h_jobs, c_jobs;
 		std::vector<std::pair<int, int>> c_launches; // rounds of the captured graph
 		cudaGraphExec_t graph = nullptr;             // the rounds of the last job table
@@ -1702,7 +1711,10 @@ struct spk_batch
 	};
 	int device = 0;
 	std::vector<spk_net *> nets;
-	group groups[2 * spk::MODEL_COUNT]; // by model id and kernel (window_flat, window_slots)
+	// by model id and kernel: window_flat, window_slots, window_plastic (one CTA per SM, up to
+	// 512 threads), window_plastic (two CTAs per SM, up to PL_THREADS threads)
+	static constexpr int KINDS = 4;
+	group groups[KINDS * spk::MODEL_COUNT];
 
 	~spk_batch()
 	{
@@ -1715,25 +1727,41 @@ struct spk_batch
 		}
 	}
 
-	// stepped by the shared window_flat_batch launches
-	static bool shared( spk_net const & net ) { return net.flat && !plastic_of( net.model ); }
+	// stepped by the shared launches (window_flat_batch, window_slots_batch,
+	// window_plastic_batch); window_counts and window_ordered nets run their own windows
+	static bool shared( spk_net const & net ) { return ( net.flat && !plastic_of( net.model ) ) || plastic_of( net.model ); }
+	static int kind( spk_net const & net )
+	{
+		if( plastic_of( net.model ) ) return net.tc.threads <= spk::PL_THREADS ? 3 : 2;
+		return net.slot_vecs ? 1 : 0;
+	}
 
 	template <typename Model>
-	static void launch_model( group & g, int4 const * jobs, int njobs, int smem, bool slotted )
+	static void launch_model( group & g, int4 const * jobs, int njobs, int smem, int kind, int threads )
 	{
+		auto const * params = g.d_params.as<spk::net_params const>();
 		if constexpr( spk::is_flat_model<Model> )
 		{
-			if( slotted )
-				spk::window_slots_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
+			if( kind == 1 )
+				spk::window_slots_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( params, jobs, smem );
 			else
-				spk::window_flat_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( g.d_params.as<spk::net_params const>(), jobs, smem );
+				spk::window_flat_batch<Model><<<njobs, spk::FLAT_THREADS, smem, g.stream>>>( params, jobs, smem );
+			CK( cudaGetLastError() );
+		}
+		else if constexpr( spk::is_plastic_model<Model> )
+		{
+			auto const * pls = g.d_pls.as<spk::plastic_params const>();
+			if( kind == 3 )
+				spk::window_plastic_batch<Model, spk::PL_CTAS_PER_SM><<<njobs, threads, smem, g.stream>>>( params, pls, jobs );
+			else
+				spk::window_plastic_batch<Model, 1><<<njobs, threads, smem, g.stream>>>( params, pls, jobs );
 			CK( cudaGetLastError() );
 		}
 	}
 
 	// advance the nets of one model by nsteps: rounds of one launch, every tile of every net
 	// running up to its own window (delay) of steps per round
-	void run_group( group & g, int model, std::vector<spk_net *> const & gn, std::vector<unsigned long long> const & counts )
+	void run_group( group & g, int model, int kind, std::vector<spk_net *> const & gn, std::vector<unsigned long long> const & counts )
 	{
 		for( auto * net : gn )
 		{
@@ -1743,6 +1771,9 @@ struct spk_batch
 		}
 		g.h_params.resize( gn.size() );
 		for( size_t i = 0; i < gn.size(); i++ ) g.h_params[i] = gn[i]->params();
+		bool const plastic = kind >= 2;
+		g.h_pls.resize( plastic ? gn.size() : 0 );
+		for( size_t i = 0; i < g.h_pls.size(); i++ ) g.h_pls[i] = gn[i]->plast.params();
 		// all rounds' jobs (net, tile, steps, dt) at once; a round whose windows equal the
 		// previous round's reuses its jobs
 		std::vector<unsigned long long> left = counts;
@@ -1776,15 +1807,18 @@ struct spk_batch
 			}
 		}
 		size_t const pb = g.h_params.size() * sizeof( spk::net_params ), jb = g.h_jobs.size() * sizeof( int4 );
-		if( g.d_params.bytes < pb || g.d_jobs.bytes < jb )
+		size_t const qb = g.h_pls.size() * sizeof( spk::plastic_params );
+		if( g.d_params.bytes < pb || g.d_jobs.bytes < jb || g.d_pls.bytes < qb )
 		{
 			CK( cudaStreamSynchronize( g.stream ) ); // launches reading the old ones
 			g.drop_graph();                          // captured the old buffers
 			g.c_params.clear();
 			g.c_jobs.clear();
+			g.c_pls.clear();
 		}
 		if( g.d_params.bytes < pb ) g.d_params.alloc( pb );
 		if( g.d_jobs.bytes < jb ) g.d_jobs.alloc( jb );
+		if( g.d_pls.bytes < qb ) g.d_pls.alloc( qb );
 		// pageable sources: each copy returns once its source is staged, and the stream
 		// orders it after the previous run's launches that read the same buffers; a table
 		// equal to the one on the device is not sent again
@@ -1802,13 +1836,26 @@ struct spk_batch
 			g.c_jobs = g.h_jobs;
 			g.drop_graph();
 		}
-		bool const slotted = gn[0]->slot_vecs > 0;
-		int const smem = slotted ? gn[0]->slot_smem : gn[0]->flat_smem;
+		if( !same( g.h_pls, g.c_pls ) )
+		{
+			CK( cudaMemcpyAsync( g.d_pls.p, g.h_pls.data(), qb, cudaMemcpyHostToDevice, g.stream ) );
+			g.c_pls = g.h_pls;
+		}
+		// launch shape: window_flat's fixed one, or the widest plastic tile and the largest
+		// shared-memory carve-up at that width
+		int threads = spk::FLAT_THREADS, smem = kind == 1 ? gn[0]->slot_smem : gn[0]->flat_smem;
+		if( plastic )
+		{
+			threads = 32;
+			for( auto * net : gn ) threads = std::max( threads, net->tc.threads );
+			smem = 0;
+			for( auto * net : gn ) smem = std::max( smem, spk::plastic_window_smem( net->tc.tile, net->tc.ntiles, threads ) );
+		}
 		auto launch_all = [&] {
 			for( auto const & l : launches )
 			{
 				int4 const * jobs = g.d_jobs.as<int4 const>() + l.first;
-				dispatch( model, [&]( auto tag ) { launch_model<typename decltype( tag )::type>( g, jobs, l.second, smem, slotted ); } );
+				dispatch( model, [&]( auto tag ) { launch_model<typename decltype( tag )::type>( g, jobs, l.second, smem, kind, threads ); } );
 			}
 		};
 		// the rounds as one CUDA graph, captured once per job table and round sequence and
@@ -1844,24 +1891,24 @@ struct spk_batch
 	// advance nets[i] by counts[i] steps (members of the batch)
 	void run( std::vector<spk_net *> const & which, std::vector<unsigned long long> const & counts )
 	{
-		// nets outside window_flat (plastic ones) run their own windows on their own
-		// streams, concurrently with the shared launches
-		std::vector<spk_net *> gn[2 * spk::MODEL_COUNT];
-		std::vector<unsigned long long> gc[2 * spk::MODEL_COUNT];
+		// nets outside the shared kernels (window_counts, window_ordered) run their own
+		// windows on their own streams, concurrently with the shared launches
+		std::vector<spk_net *> gn[KINDS * spk::MODEL_COUNT];
+		std::vector<unsigned long long> gc[KINDS * spk::MODEL_COUNT];
 		for( size_t i = 0; i < which.size(); i++ )
 		{
 			if( counts[i] == 0 ) continue;
 			if( shared( *which[i] ) )
 			{
-				int const gi = 2 * which[i]->model + ( which[i]->slot_vecs ? 1 : 0 );
+				int const gi = KINDS * which[i]->model + kind( *which[i] );
 				gn[gi].push_back( which[i] );
 				gc[gi].push_back( counts[i] );
 			}
 			else
 				which[i]->run( counts[i] );
 		}
-		for( int m = 0; m < 2 * spk::MODEL_COUNT; m++ )
-			if( !gn[m].empty() ) run_group( groups[m], m / 2, gn[m], gc[m] );
+		for( int m = 0; m < KINDS * spk::MODEL_COUNT; m++ )
+			if( !gn[m].empty() ) run_group( groups[m], m / KINDS, m % KINDS, gn[m], gc[m] );
 	}
 };
 
@@ -2642,9 +2689,11 @@ int spk_batch_add( spk_batch * b, spk_net * net )
 		require( b != nullptr && net != nullptr, "null argument" );
 		require( net->device == b->device, "the net lives on another device" );
 		require( net->batch == nullptr, "the net belongs to a batch already" );
-		if( spk_batch::shared( *net ) )
+		// window_flat's batched launches have one shared-memory size (plastic launches take
+		// theirs from their nets)
+		if( net->flat )
 			for( auto * o : b->nets )
-				require( !spk_batch::shared( *o ) || ( o->flat_smem == net->flat_smem && o->slot_smem == net->slot_smem ),
+				require( !o->flat || ( o->flat_smem == net->flat_smem && o->slot_smem == net->slot_smem ),
 				         "nets of a batch share one kernel configuration" );
 		b->nets.push_back( net );
 		net->batch = b;

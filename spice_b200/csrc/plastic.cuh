@@ -165,8 +165,10 @@ __device__ __forceinline__ void window_trace( float zrf, int rf_off, long long t
 	}
 }
 
-template <typename Model, int NPT, int CTAS>
-__global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS ) window_plastic( net_params p, plastic_params q, int L, float dt )
+// The window step of tile `tile` of a plastic net (L steps of dt): the body of
+// window_plastic and window_plastic_batch. Tiles of up to blockDim.x * NPT neurons.
+template <typename Model, int NPT>
+__device__ __forceinline__ void window_plastic_body( net_params const & p, plastic_params const & q, int const tile, int L, float dt )
 {
 	using N = typename Model::neuron;
 	using Syn = typename Model::synapse;
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS ) window_p
 
 	int const T = p.tile, tid = threadIdx.x;
 	int const warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-	int const tile = blockIdx.x, d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
+	int const d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	snn_info const info{ p.n };
 
 	// shared memory carve-up (sizes: see plastic_window_smem)
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS ) window_p
 		float c2 = c, sum2 = sum;
 		for( int k = L; k < L + p.delay; k++ ) s_dt[k] = kahan_add( c2, sum2, dt );
 		s_t0 = cs.step;
-		if( blockIdx.x == 0 )
+		if( tile == 0 )
 			for( int k = 0; k < L; k++ ) p.dt_ring[( cs.step + k ) % DT_RING] = s_dt[k];
 	}
 	__syncthreads();
@@ -588,6 +590,33 @@ __global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS ) window_p
 		}
 	}
 	window_clock_end( p, L, t0, s_c, s_sum );
+}
+
+template <typename Model, int NPT, int CTAS>
+__global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS ) window_plastic( net_params p, plastic_params q, int L, float dt )
+{
+	window_plastic_body<Model, NPT>( p, q, blockIdx.x, L, dt );
+}
+
+// Many plastic nets of one model in one launch (batching): CTA b runs tile jobs[b].y of net
+// jobs[b].x (parameters nets[], pls[]) for jobs[b].z steps of dt __int_as_float(jobs[b].w),
+// one neuron per thread. The launch has as many threads as its widest tile (at most
+// PL_THREADS for the two-CTAs-per-SM form); a narrower tile leaves the rest of its threads
+// idle. Every net's steps read only spikes of earlier launches (jobs[b].z <= its delay).
+template <typename Model, int CTAS>
+__global__ void __launch_bounds__( CTAS == 1 ? 512 : PL_THREADS, CTAS )
+    window_plastic_batch( net_params const * nets, plastic_params const * pls, int4 const * jobs )
+{
+	__shared__ net_params s_p;
+	__shared__ plastic_params s_q;
+	int4 const j = jobs[blockIdx.x];
+	if( threadIdx.x == 0 )
+	{
+		s_p = nets[j.x];
+		s_q = pls[j.x];
+	}
+	__syncthreads();
+	if( j.z > 0 ) window_plastic_body<Model, 1>( s_p, s_q, j.y, j.z, __int_as_float( j.w ) );
 }
 
 // synapse::init for every edge (pads 0), per-neuron traces at their initial value.

@@ -407,14 +407,19 @@ BATCH_NETS = [
     ("brunel", [12000, 12000], [(0, 1, 0.05), (1, 1, 0.05)], 6, 20),
     ("synth", [200_000], [(0, 0, 16 / 200_000)], 4, 12),
     ("synth", [30_000], [(0, 0, 0.001)], 15, 1),
-    ("brunel_with_plasticity", [1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 2),  # own stream
+    # plastic nets in shared window_plastic_batch launches of both forms: 128- and 224-neuron
+    # tiles (two CTAs per SM), 480-neuron tiles (one CTA per SM), another plastic model
+    ("brunel_with_plasticity", [1000, 1000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 2),
+    ("brunel_with_plasticity", [15_000, 15_000], [(0, 1, 0.02), (1, 1, 0.02)], 9, 2),
+    ("brunel_with_plasticity", [35_000, 35_000], [(0, 1, 0.01), (1, 1, 0.01)], 12, 2),
+    ("brunel_with_plasticity_a012", [2000, 2000], [(0, 1, 0.1), (1, 1, 0.1)], 7, 2),
 ]
 
 
 def test_batch_matches_nets_alone():
-    """Nets of three models, uneven sizes and delays, re-tiled and stepped by shared
-    launches (and a plastic net beside them), against each net stepped alone: state
-    bit-identical, spikes equal."""
+    """Nets of five models, uneven sizes and delays, re-tiled (window_flat nets) and stepped
+    by shared launches, plastic nets of different tile widths among them, against each net
+    stepped alone: state and weights bit-identical, spikes equal."""
     alone, batched = [], []
     batch = spice_b200.Batch()
     for i, (model, pops, conns, delay, target) in enumerate(BATCH_NETS):
