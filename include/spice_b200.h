@@ -340,12 +340,15 @@ typedef struct spk_server_stats
 	double tick_seconds;  /* ticks: batch runs until every stepped net synchronised */
 } spk_server_stats;
 
-/* Starts the builder threads (SPK_SERVER_BUILDERS, 1-8, default 2) and the ticker. The
+/* Starts the builder threads (two) and the ticker. The
  * budget (at most the device's free memory less 1 GiB) is mapped into the device's
  * stream-ordered memory pool first, and the jobs' nets are built from that pool, so
  * neither building nor freeing a net synchronises the device; creation takes about 2-3.5 s
  * for 150 GB, and spk_server_destroy hands the memory back. */
 int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps );
+/* spk_server_create with `builders` builder threads (1-8; 0 = automatic: two, or the test
+ * override SPK_SERVER_BUILDERS). */
+int spk_server_create_ex( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps, int builders );
 /* Queue a job: the arguments of spk_net_create, its number of steps and a deadline in
  * seconds from submission (0 = none). SPK_ERR_NOMEM (and a job in state REFUSED) if the
  * job alone exceeds the budget. */

@@ -179,6 +179,7 @@ def library():
         "spk_net_estimate_bytes_opts": (I, [I, P(_LayoutDesc), I, I, P(_NetOptions), P(U64)]),
         "spk_batch_run_nets": (I, [VP, I, P(VP), P(U64)]),
         "spk_server_create": (I, [P(VP), I, U64, U64]),
+        "spk_server_create_ex": (I, [P(VP), I, U64, U64, I]),
         "spk_server_submit": (I, [VP, I, P(_LayoutDesc), F, I, U64, U64, U64, C.c_double, P(U64)]),
         "spk_server_job_info": (I, [VP, U64, P(JobInfo)]),
         "spk_server_job_neurons": (I, [VP, U64, P(VP)]),
@@ -511,10 +512,11 @@ class Server:
     srv.wait(job); V, Twait = srv.neurons(job)
     """
 
-    def __init__(self, budget_bytes, quantum=1500, device=0):
+    def __init__(self, budget_bytes, quantum=1500, device=0, builders=0):
         self._h = C.c_void_p()
         self._models = {}
-        _check(library().spk_server_create(C.byref(self._h), int(device), int(budget_bytes), int(quantum)))
+        _check(library().spk_server_create_ex(C.byref(self._h), int(device), int(budget_bytes), int(quantum),
+                                              int(builders)))
 
     def submit(self, model, layout, nsteps, dt=1e-4, delay=1, seed=1, graph_seed=1337, timeout=0.0):
         """Queue a job; returns its id. Raises SpiceError (ERR_NOMEM) if it alone exceeds the budget."""

@@ -53,12 +53,17 @@ bool plastic_model( int model )
 
 namespace
 {
-// builder threads: SPK_SERVER_BUILDERS (1-8), default 2 (with jobs queued, a second
-// builder overlaps one build's host work with another's kernels)
-int builders_count()
+// builder threads: 2 unless the creator asks (1-8); with jobs queued, a second builder
+// overlaps one build's host work with another's kernels. SPK_SERVER_BUILDERS overrides the
+// automatic choice (a test hook).
+int builders_count( int requested )
 {
-	char const * e = getenv( "SPK_SERVER_BUILDERS" );
-	int const n = e ? atoi( e ) : 2;
+	int n = requested;
+	if( n <= 0 )
+	{
+		char const * e = getenv( "SPK_SERVER_BUILDERS" );
+		n = e ? atoi( e ) : 2;
+	}
 	return n < 1 ? 1 : ( n > 8 ? 8 : n );
 }
 
@@ -123,7 +128,7 @@ struct server
 	uint64_t in_use = 0, peak = 0, ticks = 0;
 	double build_s = 0, tick_s = 0;
 	int inject = 0;
-	std::vector<std::thread> builders; // builders_count() threads admit and build concurrently
+	std::vector<std::thread> builders; // builder threads: they admit and build concurrently
 	std::thread ticker;
 
 	double now() const { return std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count(); }
@@ -432,7 +437,13 @@ struct spk_server : server
 extern "C" {
 int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps )
 {
+	return spk_server_create_ex( out, device, budget_bytes, quantum_steps, 0 );
+}
+
+int spk_server_create_ex( spk_server ** out, int device, uint64_t budget_bytes, uint64_t quantum_steps, int builders )
+{
 	if( !out ) return fail( SPK_ERR_INVALID, "out is null" );
+	if( builders < 0 || builders > 8 ) return fail( SPK_ERR_INVALID, "builders must be 0 (automatic) to 8" );
 	*out = nullptr;
 	if( budget_bytes == 0 || quantum_steps == 0 ) return fail( SPK_ERR_INVALID, "budget and quantum must be > 0" );
 	auto s = std::make_unique<spk_server>();
@@ -445,7 +456,7 @@ int spk_server_create( spk_server ** out, int device, uint64_t budget_bytes, uin
 	if( rc != SPK_OK ) return rc;
 	// the budget mapped into the pool the nets are built from, before any job runs
 	spk_reserve_pool( device, budget_bytes );
-	for( int b = 0, nb = builders_count(); b < nb; b++ ) s->builders.emplace_back( [p = s.get()] { p->build_loop(); } );
+	for( int b = 0, nb = builders_count( builders ); b < nb; b++ ) s->builders.emplace_back( [p = s.get()] { p->build_loop(); } );
 	s->ticker = std::thread( [p = s.get()] { p->tick_loop(); } );
 	*out = s.release();
 	return SPK_OK;

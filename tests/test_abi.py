@@ -95,6 +95,8 @@ def test_server_and_batch_arguments_checked_without_device(lib):
     h = C.c_void_p()
     assert lib.spk_server_create(C.byref(h), 0, 0, 10) == spice_b200.ERR_INVALID  # zero budget
     assert lib.spk_server_create(None, 0, 1 << 30, 10) == spice_b200.ERR_INVALID
+    assert lib.spk_server_create_ex(C.byref(h), 0, 1 << 30, 10, 9) == spice_b200.ERR_INVALID  # builders 1-8
+    assert b"builders" in lib.spk_last_error()
     assert lib.spk_server_wait(None, 0, 0.0) == spice_b200.ERR_INVALID
     assert lib.spk_batch_run(None, 1) == spice_b200.ERR_INVALID
     assert lib.spk_batch_add(None, None) == spice_b200.ERR_INVALID
