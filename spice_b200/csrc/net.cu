@@ -314,7 +314,6 @@ spk::model_traits describe( int model )
 }
 
 bool plastic_of( int model ) { return describe( model ).plastic; }
-bool ordered_of( int model ) { return describe( model ).ordered; }
 int classes_of( int model ) { return describe( model ).classes; }
 int neuron_attrs_of( int model ) { return describe( model ).neuron_attrs; }
 
