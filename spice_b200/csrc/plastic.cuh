@@ -359,19 +359,19 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 				int const m = min( PL_STAGE, total - b0 );
 				stage_spikes( p, q, slot_in, tile, pref, b0, m, sb );
 				__syncthreads();
-				for( int c0 = 0; c0 < m; c0 += PL_CHUNK )
-				{
-					int const mc = min( PL_CHUNK, m - c0 );
-					if( tid < mc ) s_src[tid] = sb[c0 + tid].src;
-					// each warp's spikes of the chunk (x = warp, warp + nw, ...): the first two
-					// targets and weights per lane of every spike's row slice loaded before any is
-					// processed, so the rows' global loads overlap instead of running one after
-					// another
-					constexpr int PL_AHEAD = PL_CHUNK / 4; // spikes per warp, 4 warps at least
-					int pd[PL_AHEAD][2];
-					float pw[PL_AHEAD][2];
+				// chunks of `chunk` arrivals, PL_AH per warp, each with its row slice's first two
+				// elements per lane loaded ahead: a chunk's loads are issued while the chunk
+				// before it is walked and received, so their latency overlaps that work (a
+				// chunk's rows are other sources than the chunk before it: no weight it loads is
+				// one that chunk writes)
+				constexpr int PL_AH = 4;
+				int const chunk = min( PL_CHUNK, PL_AH * nw );
+				int pdA[PL_AH][2], pdB[PL_AH][2];
+				float pwA[PL_AH][2], pwB[PL_AH][2];
+				auto preload = [&]( int cc0, int( &pd )[PL_AH][2], float( &pw )[PL_AH][2] ) {
+					int const cmc = min( chunk, m - cc0 );
 #pragma unroll
-					for( int u = 0; u < PL_AHEAD; u++ )
+					for( int u = 0; u < PL_AH; u++ )
 					{
 						int const x = warp + u * nw;
 #pragma unroll
@@ -380,9 +380,9 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 							pd[u][h] = -1;
 							pw[u][h] = 0.0f;
 						}
-						if( x < mc )
+						if( x < cmc )
 						{
-							stage_e const e = sb[c0 + x];
+							stage_e const e = sb[cc0 + x];
 #pragma unroll
 							for( int h = 0; h < 2; h++ )
 							{
@@ -395,6 +395,13 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 							}
 						}
 					}
+				};
+				preload( 0, pdA, pwA );
+				for( int c0 = 0; c0 < m; c0 += chunk )
+				{
+					int const mc = min( chunk, m - c0 );
+					if( tid < mc ) s_src[tid] = sb[c0 + tid].src;
+					if( c0 + chunk < m ) preload( c0 + chunk, pdB, pwB );
 					// spike x of the chunk into its weight column; (d1st, w1st) = its first slice
 					// element if loaded ahead (ahead1st)
 					auto arrive = [&]( int x, bool ahead1st, int d1st, float w1st, int d2nd, float w2nd ) {
@@ -441,10 +448,8 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 						if( replay ) __syncwarp();
 					};
 #pragma unroll
-					for( int u = 0; u < PL_AHEAD; u++ )
-						if( warp + u * nw < mc ) arrive( warp + u * nw, true, pd[u][0], pw[u][0], pd[u][1], pw[u][1] );
-					// narrow CTAs (fewer than four warps): the rest without loads ahead
-					for( int x = warp + PL_AHEAD * nw; x < mc; x += nw ) arrive( x, false, 0, 0.0f, 0, 0.0f );
+					for( int u = 0; u < PL_AH; u++ ) // every arrival of the chunk (chunk <= PL_AH * nw)
+						if( warp + u * nw < mc ) arrive( warp + u * nw, true, pdA[u][0], pwA[u][0], pdA[u][1], pwA[u][1] );
 					__syncthreads();
 					// every target adds its inputs in ascending source order
 #pragma unroll
@@ -469,6 +474,14 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 						}
 					}
 					__syncthreads();
+#pragma unroll
+					for( int u = 0; u < PL_AH; u++ )
+#pragma unroll
+						for( int h = 0; h < 2; h++ )
+						{
+							pdA[u][h] = pdB[u][h];
+							pwA[u][h] = pwB[u][h];
+						}
 				}
 			}
 		}
