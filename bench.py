@@ -440,7 +440,7 @@ def run_batched(args, rank, world):
     del plain
 
     # (b) batch: tiles per net by work share at the scale the autotuner measured best
-    from spice_b200.autotune import autotune, layout_work, tile_targets as targets_for
+    from spice_b200.autotune import autotune, autotune_producers, layout_work, tile_targets as targets_for
 
     works = [layout_work(Layout(s["pops"], s["conns"])) for s in specs]
 
@@ -451,12 +451,15 @@ def run_batched(args, rank, world):
 
     t0 = time.perf_counter()
     scale, buckets, tune_times = autotune(build, works, sms, device=dev)
+    prod, prod_times = autotune_producers(build, works, sms, scale, buckets, device=dev)
+    tune_times.update(prod_times)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     nets = [make(s) for s in specs]
     batch = Batch(device=dev)
-    for n, t in zip(nets, targets_for(works, sms, scale, buckets)):
+    for n, t, b in zip(nets, targets_for(works, sms, scale, buckets), buckets):
         n.set_tile_target(t)
+        n.set_producer_warps(prod[b])
         batch.add(n)
     for n in nets:
         n.sync()
@@ -482,7 +485,7 @@ def run_batched(args, rank, world):
                 "config": {"workload": f"batched_{len(specs)}_nets", "nets": counts, "synapses_total": syn_total,
                            "syn_range": [1e5, 5e7], "bio_s_per_net": steps * DT, "dt": DT, "tiles_total": tiles},
                 "batch": {"wall_s": wall_batch, "wall_per_bio": wall_batch / bio_total, "setup_s": setup_batch,
-                          "tile_scale": scale, "autotune_s": tune_s,
+                          "tile_scale": scale, "producer_warps": prod, "autotune_s": tune_s,
                           "autotune_ms_per_step": {k: v * 1e3 for k, v in tune_times.items()}},
                 "plain_loop": {"wall_s": wall_plain, "wall_per_bio": wall_plain / bio_total, "setup_s": setup_plain,
                                "wall_s_by_model": per_model,

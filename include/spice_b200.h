@@ -280,6 +280,13 @@ typedef struct spk_batch spk_batch;
  * the GPU with others in a batch takes fewer CTAs than a net alone (one per SM). */
 int spk_net_set_tile_target( spk_net * net, int target );
 
+/* window_flat's split of its 32 warps: `warps` (4-24, default 12) stage the next steps'
+ * arrivals and copy their slices (the last of them compacts and publishes the tile's
+ * spikes), the rest count arrivals and update neurons. A tuning choice for nets of
+ * different sizes (the batch autotuner sets it per size bucket); results do not depend on
+ * it. Nets of the other kernels ignore it. */
+int spk_net_set_producer_warps( spk_net * net, int warps );
+
 int spk_batch_create( spk_batch ** out, int device );
 /* Nets of any model, on the batch's device; a net belongs to at most one batch. The nets
  * of one model share launches (window_flat_batch, window_slots_batch, window_plastic_batch:

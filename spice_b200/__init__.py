@@ -170,6 +170,7 @@ def library():
         "spk_net_synapses": (I, [VP, P(VP)]),
         "spk_model_attrs": (I, [I, P(I), P(I), C.c_char_p, I]),
         "spk_net_set_tile_target": (I, [VP, I]),
+        "spk_net_set_producer_warps": (I, [VP, I]),
         "spk_net_checkpoint": (I, [VP, VP, U64, P(U64)]),
         "spk_net_restore": (I, [P(VP), VP, U64, I]),
         "spk_net_create_ex": (I, [P(VP), I, P(_LayoutDesc), F, I, U64, U64, I, I]),
@@ -434,6 +435,10 @@ class Snn:
         net.model = MODEL_NAMES[net.info().model]
         net._ndt, net._sdt = model_attrs(net.model)
         return net
+
+    def set_producer_warps(self, warps):
+        """window_flat's producer warps (4-24, default 12): a tuning choice, same results."""
+        _check(library().spk_net_set_producer_warps(self._h, int(warps)))
 
     def set_tile_target(self, target):
         """Re-tile (before the first step) into about `target` tiles, for sharing the GPU."""

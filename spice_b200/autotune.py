@@ -8,14 +8,16 @@ waves per launch. The rule here gives net i a share of the SMs by its expected w
 
 with one scale per size bucket b (nets split into buckets by work), and `autotune`
 measures scales on the nets themselves (or a sample of them spread over their size range):
-first one scale for all, then each bucket's scale in turn with the others held. Results
-never depend on the tiling: only the speed does.
+first one scale for all, then each bucket's scale in turn with the others held.
+`autotune_producers` then chooses, per bucket, how many of window_flat's 32 warps stage and
+copy the next steps' arrivals (the rest count and update). Results never depend on the
+tiling or the split: only the speed does.
 """
 import time
 
 import numpy as np
 
-__all__ = ["layout_work", "tile_targets", "size_buckets", "autotune"]
+__all__ = ["layout_work", "tile_targets", "size_buckets", "autotune", "autotune_producers"]
 
 
 def layout_work(layout):
@@ -53,7 +55,7 @@ def _sample(works, max_nets):
     return sorted(set(int(order[k]) for k in picks))
 
 
-def _measure(build, idx, targets, w_all, steps, warmup, device):
+def _measure(build, idx, targets, w_all, steps, warmup, device, producers=None):
     from . import Batch
 
     nets = []
@@ -61,6 +63,8 @@ def _measure(build, idx, targets, w_all, steps, warmup, device):
     try:
         for i in idx:
             net = build(i, targets[i])
+            if producers is not None:
+                net.set_producer_warps(producers[i])
             nets.append(net)
             batch.add(net)
         batch.run(warmup)
@@ -109,3 +113,31 @@ def autotune(build, works, sms, scales=(0.5, 1.0, 2.0, 4.0), nbuckets=3, steps=1
         cands = [best[:b] + [s] + best[b + 1:] for s in scales]
         best = min(cands, key=run)
     return best, buckets, times
+
+
+def autotune_producers(build, works, sms, scale, buckets, producers=(8, 12, 16), steps=150, warmup=30, max_nets=64,
+                       device=0):
+    """window_flat's producer warps per size bucket, measured on the batch tiled by
+    (scale, buckets) as `autotune` chose: each bucket's count in turn over the candidates,
+    the other buckets held (at 12, then at their choice). Returns (per-bucket producer warps,
+    {description: seconds per step})."""
+    idx = _sample(works, max_nets)
+    nb = max(buckets) + 1 if buckets else 1
+    targets = tile_targets(works, sms, scale, buckets)
+    w_all = float(sum(works)) or 1.0
+    w_sub = float(sum(works[i] for i in idx)) or 1.0
+    times = {}
+
+    def run(pr):
+        key = "producers " + "/".join(str(x) for x in pr)
+        if key not in times:
+            t = _measure(build, idx, targets, w_all, steps, warmup, device, [pr[buckets[i]] for i in range(len(works))])
+            times[key] = t / steps * (w_all / w_sub)
+        return times[key]
+
+    best = [12] * nb
+    for b in range(nb):
+        if not any(buckets[i] == b for i in idx):
+            continue
+        best = min((best[:b] + [x] + best[b + 1:] for x in producers), key=run)
+    return best, times

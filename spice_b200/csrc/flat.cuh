@@ -46,7 +46,9 @@ constexpr int FLAT_THREADS = 1024;    // threads of a window_flat CTA (one CTA p
 #ifndef SPK_FLAT_PRODUCERS
 #define SPK_FLAT_PRODUCERS 12
 #endif
-constexpr int FLAT_PRODUCERS = SPK_FLAT_PRODUCERS; // warps that stage, copy slices and compact spikes
+constexpr int FLAT_PRODUCERS = SPK_FLAT_PRODUCERS; // warps that stage, copy slices and compact spikes (default)
+constexpr int FLAT_MIN_PRODUCERS = 4;  // two scanning warps and the publisher at least
+constexpr int FLAT_MAX_PRODUCERS = 24; // eight consumer warps at least
 constexpr int FLAT_PC = 1032;         // per-source-tile counts of one step (ntiles + 1 <= FLAT_PC)
 constexpr int FLAT_STEP_CAP = 1024;   // arrivals of one step the pipeline stages
 constexpr int FLAT_ENT_CAP = 6144;    // arrivals per segment of the synchronous path
@@ -503,9 +505,9 @@ __device__ __forceinline__ void count_buffer( uint4 const * buf, int V, unsigned
 
 // barrier of the first `threads` threads (whole warps) of the CTA
 __device__ __forceinline__ void bar_sync_first( int threads ) { asm volatile( "bar.sync 1, %0;\n" ::"r"( threads ) : "memory" ); }
-// barrier of the producer warps (FLAT_PRODUCERS - 1 warps before the last one, which
-// compacts and publishes)
-__device__ __forceinline__ void bar_sync_producers() { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * ( FLAT_PRODUCERS - 1 ) ) : "memory" ); }
+// barrier of the producer warps (producers - 1 warps before the last one, which compacts
+// and publishes)
+__device__ __forceinline__ void bar_sync_producers( int producers ) { asm volatile( "bar.sync 2, %0;\n" ::"r"( 32 * ( producers - 1 ) ) : "memory" ); }
 
 // ascending compaction of a step's fired bits into the spike ring, by one warp: 32 words
 // per round, a warp scan of their counts gives every word's offset; then the step is
@@ -636,7 +638,7 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 	__shared__ int m_e[8], m_v[8], m_off[8], m_big[8];
 
 	int const tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-	int const nwc = nw - FLAT_PRODUCERS, ncons = nwc * 32; // consumer warps first, then producers
+	int const nwc = nw - p.producers, ncons = nwc * 32; // consumer warps first, then producers
 	int const d0 = __ldg( p.tile_first + tile ), d1 = __ldg( p.tile_first + tile + 1 ), span = d1 - d0;
 	int const words = ( span + 31 ) >> 5;
 	bool const inputs = __ldg( p.tile_inputs + tile ) != 0; // else no arrival ever reaches the tile
@@ -834,7 +836,7 @@ __device__ __forceinline__ void window_flat_body( net_params const & p, int cons
 				if( all )
 					__syncthreads();
 				else
-					bar_sync_producers();
+					bar_sync_producers( p.producers );
 				// the two scans, one warp each, while another producer warp compacts
 				int const pw = pt >> 5;
 				if( do_b && pw == 0 )

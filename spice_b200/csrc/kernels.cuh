@@ -70,6 +70,7 @@ struct net_params
 	int const * tile_inputs; // [ntiles] 1 if the tile has incoming synapses (window_flat)
 	int pack;                // indices per 16-byte slice vector: 8 (16-bit) or 12 (10-bit)
 	int flat_sync;           // window_flat: every step on the synchronous path
+	int producers;           // window_flat: producer warps, the publisher included (the rest count and update)
 	long long * done_step;   // [ntiles] last step whose spikes the tile has published
 	int wait_limit;          // polls of a bounded wait before it gives up (WAIT_LIMIT)
 	int withhold_tile;       // failure-detection tests: this tile never publishes (-1: none)

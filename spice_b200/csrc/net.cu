@@ -501,6 +501,7 @@ struct spk_net
 	dbuf slices, slice_rec; // tile-major 16-bit slices, [n][ntiles] records
 	dbuf tile_inputs;       // [ntiles] tiles with incoming synapses
 	int flat_sync = 0;      // window_flat without its step pipeline (opts.flat_sync)
+	int producers = spk::FLAT_PRODUCERS; // window_flat's producer warps (spk_net_set_producer_warps)
 	int pack = 8;           // slice indices per 16-byte vector: 8 (16-bit) or 12 (10-bit)
 	dbuf done_step;         // [ntiles] last step each tile has published (window_flat)
 	// window_slots (10-bit nets whose slices fit fixed slots, section on slots in slots.cuh):
@@ -550,6 +551,7 @@ struct spk_net
 		p.slice_rec = slice_rec.as<uint2 const>();
 		p.tile_inputs = tile_inputs.as<int const>();
 		p.flat_sync = flat_sync;
+		p.producers = producers;
 		p.pack = pack;
 		p.done_step = done_step.as<long long>();
 		p.wait_limit = wait_limit;
@@ -2651,6 +2653,19 @@ extern "C" int spk_generate_adj_list_static( void * stream, spk_layout_desc cons
 }
 
 extern "C" {
+int spk_net_set_producer_warps( spk_net * net, int warps )
+{
+	return guarded( [&] {
+		require( net != nullptr, "net is null" );
+		require( warps >= spk::FLAT_MIN_PRODUCERS && warps <= spk::FLAT_MAX_PRODUCERS, "producer warps must be 4 to 24" );
+		device_guard g( net->device );
+		net->flush(); // launches already queued keep the split they were captured with
+		net->producers = warps;
+		if( net->graph ) cudaGraphExecDestroy( net->graph ); // captured the old parameters
+		net->graph = nullptr;
+	} );
+}
+
 int spk_net_set_tile_target( spk_net * net, int target )
 {
 	return guarded( [&] {

@@ -99,6 +99,7 @@ def test_server_and_batch_arguments_checked_without_device(lib):
     assert b"builders" in lib.spk_last_error()
     assert lib.spk_server_wait(None, 0, 0.0) == spice_b200.ERR_INVALID
     assert lib.spk_batch_run(None, 1) == spice_b200.ERR_INVALID
+    assert lib.spk_net_set_producer_warps(None, 12) == spice_b200.ERR_INVALID
     assert lib.spk_batch_add(None, None) == spice_b200.ERR_INVALID
     assert lib.spk_server_destroy(None) == spice_b200.OK
     assert lib.spk_batch_destroy(None) == spice_b200.OK

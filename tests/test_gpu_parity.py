@@ -537,8 +537,34 @@ def test_ten_bit_slices_match_sixteen_bit(model, pops, conns, delay):
         assert bits_equal(x, y)
 
 
+@pytest.mark.parametrize("warps", [4, 7, 24])
+def test_producer_warps_do_not_change_results(warps):
+    """window_flat with 4, 7 or 24 producer warps (the autotuner's choice) against the
+    default 12: persistent recording runs, windowed steps and a batch, bit for bit."""
+    layout = Layout([10_000, 10_000], [(0, 1, 0.05), (1, 1, 0.05)])
+    a = Snn("brunel", layout, delay=15, seed=6, graph_seed=6)
+    b = Snn("brunel", layout, delay=15, seed=6, graph_seed=6)
+    b.set_producer_warps(warps)
+    ca, ia = a.run_record(400, cap=20_000 * 400 // 4)
+    cb, ib = b.run_record(400, cap=20_000 * 400 // 4)
+    assert ca.sum() > 0 and np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    for k in range(20):
+        assert np.array_equal(a.step(out=True), b.step(out=True)), k
+    c = Snn("brunel", layout, delay=15, seed=6, graph_seed=6)
+    c.set_tile_target(40)
+    c.set_producer_warps(warps)
+    batch = spice_b200.Batch()
+    batch.add(c)
+    batch.run(420)
+    for x, y in zip(a.neurons(), c.neurons()):
+        assert bits_equal(x, y)
+    with pytest.raises(spice_b200.InvalidArgument):
+        b.set_producer_warps(25)
+    batch.close()
+
+
 def test_autotune_measures_every_scale():
-    from spice_b200.autotune import autotune, layout_work
+    from spice_b200.autotune import autotune, autotune_producers, layout_work
 
     lays = [Layout([n, n], [(0, 1, 0.1), (1, 1, 0.1)]) for n in (500, 1500, 4000)]
     works = [layout_work(l) for l in lays]
@@ -551,6 +577,8 @@ def test_autotune_measures_every_scale():
     best, buckets, times = autotune(build, works, 148, scales=(0.5, 2.0), nbuckets=3, steps=45, warmup=15)
     assert len(best) == 3 and all(s in (0.5, 2.0) for s in best) and sorted(buckets) == [0, 1, 2]
     assert "0.5/0.5/0.5" in times and "2/2/2" in times and all(v > 0 for v in times.values())
+    prod, ptimes = autotune_producers(build, works, 148, best, buckets, producers=(6, 18), steps=45, warmup=15)
+    assert len(prod) == 3 and all(x in (6, 12, 18) for x in prod) and len(ptimes) >= 4
 
 
 # ----------------------------------------------------------------------- checkpoints
