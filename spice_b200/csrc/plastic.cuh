@@ -463,11 +463,29 @@ __device__ __forceinline__ void window_plastic_body( net_params const & p, plast
 							{
 								reg_iter<Tup> it{ st[kk], (uint32_t)( i0 + kk ) };
 								device_backend bak( p.seed, (uint32_t)( i0 + kk ), (uint32_t)t );
+								// four arrivals at a time: their weights loaded together, then the
+								// receives in ascending source order (the loads and the parts of
+								// receive that do not touch the neuron's state overlap)
 								while( mm )
 								{
-									int const b = __ffs( mm ) - 1;
-									mm &= mm - 1;
-									N::receive( s_src[b], it, weight_iter{ wT[b * T + local] }, info, bak );
+									constexpr int RX = 4;
+									int bs[RX];
+									float ws[RX];
+									int nb = 0;
+#pragma unroll
+									for( int u = 0; u < RX; u++ )
+										if( mm )
+										{
+											bs[u] = __ffs( mm ) - 1;
+											mm &= mm - 1;
+											nb = u + 1;
+										}
+#pragma unroll
+									for( int u = 0; u < RX; u++ )
+										if( u < nb ) ws[u] = wT[bs[u] * T + local];
+#pragma unroll
+									for( int u = 0; u < RX; u++ )
+										if( u < nb ) N::receive( s_src[bs[u]], it, weight_iter{ ws[u] }, info, bak );
 								}
 								mask[local] = 0;
 							}
