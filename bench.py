@@ -39,7 +39,12 @@ MODEL_WORKLOADS = {
     "brunel_plus": ("brunel_with_plasticity", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8),
     "brunel_plus_a012": ("brunel_with_plasticity_a012", [50000, 50000], [(0, 1, 0.1), (1, 1, 0.1)], 15, 5e8),
     "brunel_fixed": ("brunel_fixed", [70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1e9),
+    # the generic kernel (window_ordered: every arrival through receive(), in order) on nets
+    # the counting kernels also run, for comparison with the va and --syn 1e8 lines
+    "va_ordered": ("vogels_abbott", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02),
+    "brunel_ordered": ("brunel", [22360, 22360], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1e8),
 }
+WORKLOAD_OPTIONS = {"va_ordered": {"kernel": "ordered"}, "brunel_ordered": {"kernel": "ordered"}}
 
 
 def parse():
@@ -56,7 +61,8 @@ def parse():
                     help="brunel: the 1e9 headline; batched: many small nets, batch vs plain per-net loop; "
                          "serving: Poisson job arrivals, server vs plain per-job loop; va: Vogels-Abbott 4000+1000 "
                          "at delay 1; brunel_plus: Brunel with STDP at 5e8 synapses; va_ns, brunel_fixed, "
-                         "brunel_plus_a012: the same with the benchmark configurations' model constants")
+                         "brunel_plus_a012: the same with the benchmark configurations' model constants; "
+                         "va_ordered, brunel_ordered: VA and Brunel 1e8 on the generic window_ordered kernel")
     ap.add_argument("--duration", type=float, default=8.0, help="serving: seconds of job arrivals")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: job arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
@@ -619,7 +625,9 @@ def run_model_workload(args, rank, world):
     model, pops, conns, delay, syn = MODEL_WORKLOADS[args.workload]
     steps = int(round(args.bio / DT))
     t0 = time.perf_counter()
-    net = Snn(model, Layout(pops, conns), dt=DT, delay=delay, seed=1 + rank, graph_seed=1337 + rank, device=dev)
+    options = WORKLOAD_OPTIONS.get(args.workload)
+    net = Snn(model, Layout(pops, conns), dt=DT, delay=delay, seed=1 + rank, graph_seed=1337 + rank, device=dev,
+              options=options)
     net.sync()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(net.stream(), device=dev)
@@ -641,7 +649,8 @@ def run_model_workload(args, rank, world):
     e2e = max_over_ranks(time.perf_counter() - t, world)
     info = net.info()
     net.close()
-    line = {"metric": f"wall/bio time ratio, {model}", "value": ms / 1e3 / (steps * DT), "unit": "wall_s/bio_s",
+    kernel = " on window_ordered" if options and options.get("kernel") == "ordered" else ""
+    line = {"metric": f"wall/bio time ratio, {model}{kernel}", "value": ms / 1e3 / (steps * DT), "unit": "wall_s/bio_s",
             "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "neurons": sum(pops), "synapses": syn, "delay": delay, "dt": DT,
