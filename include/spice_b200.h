@@ -154,6 +154,7 @@ typedef struct spk_net_options
 {
     int tile_target; /* window_flat tiles: about this many; 0 = one per SM */
     int kernel;      /* SPK_KERNEL: 0 = window kernels (window_flat where the model allows), 1 = window_counts ("direct"),
+                        automatic: window_flat, except window_counts at delay 1 for nets of at most 1e7 synapses,
                         2 = window_ordered ("ordered": the generic kernel, every arrival through the model's receive()
                         in the reference CPU simulator's order; the only kernel of models without input classes or with
                         synapse attributes, and of no plastic model) */

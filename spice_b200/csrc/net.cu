@@ -404,6 +404,7 @@ struct build_opts
 {
 	int tile_target = 0;   // 0: one tile per SM
 	bool direct = false;   // per-step kernels instead of the window kernels
+	bool kernel_auto = true; // the kernel is the automatic choice (no field value, no test override)
 	bool ordered = false;  // the generic window_ordered kernel for any non-plastic model
 	bool pack16 = false;   // 16-bit slice indices even where 10-bit ones fit
 	bool uniform = false;  // equal tiles instead of cost-balanced ones
@@ -436,6 +437,7 @@ build_opts resolve_opts( spk_net_options const * o )
 	char const * ke = getenv( "SPK_KERNEL" );
 	int const kernel = d.kernel >= 0 ? d.kernel : !ke ? 0 : !strcmp( ke, "direct" ) ? 1 : !strcmp( ke, "ordered" ) ? 2 : 0;
 	r.direct = kernel == 1;
+	r.kernel_auto = d.kernel < 0 && !ke;
 	r.ordered = kernel == 2;
 	r.pack16 = d.slice_bits >= 0 ? d.slice_bits == 16 : env_is( "SPK_PACK", "16" );
 	r.uniform = pick( d.tiling, "SPK_TILES", "uniform", "balanced", false );
@@ -776,7 +778,7 @@ struct spk_net
 	void grow_ring( int slots )
 	{
 		if( slots <= ring_slots ) return;
-		require( flat && !plastic_of( model ) && launched == steps, "ring growth of a window_flat net between runs" );
+		require( !plastic_of( model ) && launched == steps, "ring growth of a non-plastic net between runs" );
 		dbuf ids, cnt;
 		ids.alloc( (size_t)slots * n * 4, mem() );
 		cnt.alloc( (size_t)slots * tc.ntiles * 4, mem() );
@@ -935,6 +937,27 @@ std::vector<cost_segment> layout_costs( spice::util::layout const & l )
 	}
 	return segs;
 }
+
+// synapses of a net from its cost segments (each neuron's in-degree above the update cost)
+double segment_synapses( std::vector<cost_segment> const & segs, long long n )
+{
+	double syn = 0;
+	for( size_t i = 0; i < segs.size(); i++ )
+	{
+		long long const end = i + 1 < segs.size() ? segs[i + 1].start : n;
+		syn += (double)( end - segs[i].start ) * ( segs[i].cost - UPDATE_COST );
+	}
+	return syn;
+}
+
+// The automatic kernel of a net with input classes at delay 1: window_counts (one launch
+// per step from a CUDA graph) for nets of up to this many synapses, window_flat above. At
+// delay 1 window_flat's persistent launch waits for every tile's spikes each step, about
+// 9 us; measured on B200, 1e4-step runs: VA 5,000 and 20,000 neurons 6.3 / 6.7 us per
+// step with window_counts against 8.8 / 9.3 us, Brunel 20,000 (2e7 synapses) 10.0 against
+// 9.9 us, Brunel 1e8 22.8 against 11.1 us. At delay 3 and above window_flat is as fast or
+// faster throughout.
+constexpr double PER_STEP_MAX_SYNAPSES = 1e7;
 
 // exact in-degree of every neuron of an imported ELL graph (edges already validated)
 std::vector<cost_segment> adjacency_costs( int const * edges, long long n, long long width )
@@ -1135,7 +1158,8 @@ void allocate( spk_net & net, long long n, long long width, std::vector<cost_seg
 	}
 	net.flat = false;
 	int const target = net.opts.tile_target;
-	if( !md.plastic && !net.ordered && !net.opts.direct ) flat_tiling( net, segs, target > 0 ? target : dev_sms );
+	bool const per_step = net.opts.kernel_auto && net.delay == 1 && segment_synapses( segs, n ) <= PER_STEP_MAX_SYNAPSES;
+	if( !md.plastic && !net.ordered && !net.opts.direct && !per_step ) flat_tiling( net, segs, target > 0 ? target : dev_sms );
 	if( !net.flat ) set_tiles( net, uniform_tiles( n, net.tc.tile ) );
 	net.ring_slots = 2 * net.delay;
 	allocate_buffers( net );
@@ -1405,7 +1429,9 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 	{
 		std::vector<int> first;
 		int span = 0;
-		if( !o.direct && plan_flat( model, device, n, layout_costs( l ), o.tile_target > 0 ? o.tile_target : sms, o, first, span, pack ) )
+		std::vector<cost_segment> const segs = layout_costs( l );
+		bool const per_step = o.kernel_auto && delay == 1 && segment_synapses( segs, n ) <= PER_STEP_MAX_SYNAPSES;
+		if( !o.direct && !per_step && plan_flat( model, device, n, segs, o.tile_target > 0 ? o.tile_target : sms, o, first, span, pack ) )
 		{
 			flat = true;
 			T = (long long)first.size() - 1;
@@ -2225,10 +2251,12 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 		if( net->rec_ids.bytes < std::max<uint64_t>( ids_cap, 1 ) * 4 ) net->rec_ids.alloc( std::max<uint64_t>( ids_cap, 1 ) * 4, net->mem() );
 		if( net->rec_cnt.bytes < nsteps * 4 ) net->rec_cnt.alloc( nsteps * 4, net->mem() );
 		CK( cudaMemsetAsync( net->cursor.p, 0, 8, net->stream ) );
-		// persistent nets record in chunks: one launch per chunk into a ring enlarged to
-		// hold the chunk (bounded to RECORD_RING_BYTES), one gather per chunk
+		// non-plastic nets record in chunks: a chunk's steps (one persistent launch, or its
+		// windows replayed from a CUDA graph) into a ring enlarged to hold the chunk (bounded
+		// to RECORD_RING_BYTES), then one gather per chunk; plastic nets, whose lazy-STDP
+		// rings have 2 delay slots, gather every window
 		long long chunk = 0;
-		if( net->persistent )
+		if( !plastic_of( net->model ) )
 		{
 			long long const per_slot = net->n * 4 + (long long)net->tc.ntiles * 4;
 			long long const fit = RECORD_RING_BYTES / per_slot - 2LL * net->delay;
@@ -2240,11 +2268,18 @@ int spk_net_run_record( spk_net * net, uint64_t nsteps, uint32_t * counts, int32
 		while( done < nsteps )
 		{
 			int const L = (int)std::min<uint64_t>( nsteps - done, chunk > 0 ? (uint64_t)chunk : (uint64_t)net->max_window() );
-			net->steps += L;
-			if( chunk > 0 ) net->launch_persistent( L );
-			else net->launch_window( L );
-			net->launched += L;
-			net->kernel_launches++;
+			if( chunk > 0 && !net->persistent )
+				net->run( L ); // the chunk's windows (counted there)
+			else
+			{
+				net->steps += L;
+				if( chunk > 0 )
+					net->launch_persistent( L );
+				else
+					net->launch_window( L );
+				net->launched += L;
+				net->kernel_launches++;
+			}
 			net->gather( L, net->rec_ids.as<int>(), net->rec_cnt.as<unsigned>(), ids_cap, (long long)done );
 			done += L;
 		}

@@ -82,11 +82,17 @@ def test_vogels_abbott_config_size_matches_oracle():
     va workload, 1,000 steps from the start against the restatement and 500 more from a
     mid-run hand-over to the reference."""
     pops, conns = [5000], [(0, 0, 0.02)]
-    net = Snn("vogels_abbott", Layout(pops, conns), dt=1e-4, delay=1, seed=1, graph_seed=1337)
+    # window_flat's persistent synchronous path (the automatic choice at this size and delay
+    # is window_counts: checked against it below)
+    net = Snn("vogels_abbott", Layout(pops, conns), dt=1e-4, delay=1, seed=1, graph_seed=1337, options={"kernel": "window"})
     assert net.info().persistent == 1
+    auto = Snn("vogels_abbott", Layout(pops, conns), dt=1e-4, delay=1, seed=1, graph_seed=1337)
+    assert auto.info().persistent == 0 and auto.info().slice_pack == 0
+    ac, ai = auto.run_record(1000)
     edges, width = net.adj()
     ref = oracle.OracleNet("vogels_abbott", pops, conns, delay=1, seed=1, edges=edges, width=width)
     counts, ids = net.run_record(1000)
+    assert np.array_equal(counts, ac) and np.array_equal(ids, ai)
     for k, a in enumerate(split(counts, ids)):
         assert np.array_equal(a, ref.step()), f"raster differs at step {k}"
     for a, b in zip(net.neurons(), ref.neurons()):

@@ -389,8 +389,9 @@ def test_persistent_run_matches_windows(model, pops, conns, delay, steps):
     """run() as one cooperative launch in which tiles wait for each other's published
     spikes, against the same steps as windowed launches (checked against the oracle above)."""
     layout = Layout(pops, conns)
-    a = Snn(model, layout, delay=delay, seed=5, graph_seed=11)
-    b = Snn(model, layout, delay=delay, seed=5, graph_seed=11, options={"persistent": False})
+    a = Snn(model, layout, delay=delay, seed=5, graph_seed=11, options={"kernel": "window"})
+    b = Snn(model, layout, delay=delay, seed=5, graph_seed=11, options={"kernel": "window", "persistent": False})
+    assert a.info().persistent == 1
     a.run(steps)
     b.run(steps)
     for x, y in zip(a.neurons(), b.neurons()):
