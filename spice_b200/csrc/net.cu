@@ -1739,8 +1739,10 @@ struct spk_batch
 	int device = 0;
 	std::vector<spk_net *> nets;
 	// by model id and kernel: window_flat, window_slots, window_plastic (one CTA per SM, up to
-	// 512 threads), window_plastic (two CTAs per SM, up to PL_THREADS threads)
-	static constexpr int KINDS = 4;
+	// 512 threads), then window_plastic in its two-CTAs-per-SM form for tiles of 257 to
+	// PL_THREADS, up to 128 and 129 to 256 neurons (a launch is as wide as its widest tile:
+	// narrow tiles in narrow launches, so several of their CTAs share an SM)
+	static constexpr int KINDS = 6;
 	group groups[KINDS * spk::MODEL_COUNT];
 
 	~spk_batch()
@@ -1759,7 +1761,11 @@ struct spk_batch
 	static bool shared( spk_net const & net ) { return ( net.flat && !plastic_of( net.model ) ) || plastic_of( net.model ); }
 	static int kind( spk_net const & net )
 	{
-		if( plastic_of( net.model ) ) return net.tc.threads <= spk::PL_THREADS ? 3 : 2;
+		if( plastic_of( net.model ) )
+		{
+			int const w = net.tc.threads;
+			return w <= 128 ? 4 : w <= 256 ? 5 : w <= spk::PL_THREADS ? 3 : 2;
+		}
 		return net.slot_vecs ? 1 : 0;
 	}
 
@@ -1778,7 +1784,7 @@ struct spk_batch
 		else if constexpr( spk::is_plastic_model<Model> )
 		{
 			auto const * pls = g.d_pls.as<spk::plastic_params const>();
-			if( kind == 3 )
+			if( kind >= 3 )
 				spk::window_plastic_batch<Model, spk::PL_CTAS_PER_SM><<<njobs, threads, smem, g.stream>>>( params, pls, jobs );
 			else
 				spk::window_plastic_batch<Model, 1><<<njobs, threads, smem, g.stream>>>( params, pls, jobs );
