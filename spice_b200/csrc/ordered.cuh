@@ -24,6 +24,7 @@ namespace spk
 constexpr int ORD_CHUNK = 32;
 constexpr int ORD_STAGE = 256;     // staged arrivals per batch
 constexpr int ORD_MAX_TILE = 1024; // neurons per tile (2 per thread at most)
+constexpr int ORD_AHEAD = 8;       // arrivals per warp of a chunk with their rows loaded ahead (4 warps cover a chunk)
 
 // attribute I of the synapse at edge position e (the reference's synapse id src * width + j,
 // spice/util/adj_list.cpp:40-46), in the net's structure-of-arrays synapse attributes
@@ -108,13 +109,34 @@ __global__ void __launch_bounds__( 512, 1 ) window_ordered( net_params p, int L,
 				{
 					int const mc = min( ORD_CHUNK, m - c0 );
 					if( tid < mc ) s_src[tid] = sb[c0 + tid].x;
-					for( int x = warp; x < mc; x += nw )
+					// the warp's arrivals of the chunk (x = warp, warp + nw, ...): the first two
+					// targets per lane of each row slice loaded before any is recorded, so the
+					// rows' loads overlap; the rest of a longer slice is loaded as it is walked
+					int pd[ORD_AHEAD][2];
+#pragma unroll
+					for( int u = 0; u < ORD_AHEAD; u++ )
 					{
+						int const x = warp + u * nw;
+						pd[u][0] = pd[u][1] = -1;
+						if( x < mc )
+						{
+							int4 const e = sb[c0 + x];
+#pragma unroll
+							for( int h = 0; h < 2; h++ )
+							{
+								int const j = e.y + lane + 32 * h;
+								if( j < e.z ) pd[u][h] = __ldg( p.edges + (long long)e.x * p.width + j );
+							}
+						}
+					}
+					auto record = [&]( int x, bool ahead, int d1st, int d2nd ) {
 						int4 const e = sb[c0 + x];
 						int const * row = p.edges + (long long)e.x * p.width;
 						for( int j = e.y + lane; j < e.z; j += 32 )
 						{
-							int const local = __ldg( row + j ) - d0;
+							int const it = ( j - e.y - lane ) >> 5;
+							int const d = ahead && it < 2 ? ( it == 0 ? d1st : d2nd ) : __ldg( row + j );
+							int const local = d - d0;
 							if( (unsigned)local >= (unsigned)span )
 							{
 								atomicOr( p.err, ERR_BAD_TARGET );
@@ -123,7 +145,11 @@ __global__ void __launch_bounds__( 512, 1 ) window_ordered( net_params p, int L,
 							pos[x * T + local] = j;
 							atomicOr( mask + local, 1u << x );
 						}
-					}
+					};
+#pragma unroll
+					for( int u = 0; u < ORD_AHEAD; u++ )
+						if( warp + u * nw < mc ) record( warp + u * nw, true, pd[u][0], pd[u][1] );
+					for( int x = warp + ORD_AHEAD * nw; x < mc; x += nw ) record( x, false, 0, 0 ); // CTAs of < 4 warps
 					__syncthreads();
 					// every target applies its arrivals of the chunk in ascending source order
 #pragma unroll
@@ -136,12 +162,28 @@ __global__ void __launch_bounds__( 512, 1 ) window_ordered( net_params p, int L,
 						mask[local] = 0u;
 						reg_iter<Tup> it{ st[q], (uint32_t)( i0 + q ) };
 						device_backend bak( p.seed, (uint32_t)( i0 + q ), (uint32_t)t );
+						// four arrivals at a time, in ascending source order: their synapses'
+						// attribute loads (inside receive) are independent of each other
 						while( mm )
 						{
-							int const b = __ffs( mm ) - 1;
-							mm &= mm - 1;
-							int const src = s_src[b];
-							N::receive( src, it, syn_ref_iter<S, false>{ p.syn_attr, (long long)src * p.width + pos[b * T + local] }, info, bak );
+							constexpr int RX = 4;
+							int bs[RX];
+							int nb = 0;
+#pragma unroll
+							for( int u = 0; u < RX; u++ )
+								if( mm )
+								{
+									bs[u] = __ffs( mm ) - 1;
+									mm &= mm - 1;
+									nb = u + 1;
+								}
+#pragma unroll
+							for( int u = 0; u < RX; u++ )
+								if( u < nb )
+								{
+									int const src = s_src[bs[u]];
+									N::receive( src, it, syn_ref_iter<S, false>{ p.syn_attr, (long long)src * p.width + pos[bs[u] * T + local] }, info, bak );
+								}
 						}
 					}
 					__syncthreads();
