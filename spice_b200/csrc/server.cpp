@@ -243,9 +243,10 @@ struct server
 				spk_net_info info{};
 				if( spk_net_get_info( j->net, &info ) == SPK_OK && spk_batch_add( batch, j->net ) == SPK_OK )
 				{
-					// nets outside the shared launches run on their own streams, each at its
-					// own pace: the ticks of the shared launches do not wait for them
-					j->own = plastic_model( info.model ) || info.slice_pack == 0;
+					// nets outside the shared launches (window_counts, window_ordered) run on
+					// their own streams, each at its own pace: the ticks of the shared
+					// launches do not wait for them; plastic nets share window_plastic_batch
+					j->own = !plastic_model( info.model ) && info.slice_pack == 0;
 					running_t.push_back( j );
 				}
 				else
