@@ -41,10 +41,17 @@ MODEL_WORKLOADS = {
     "brunel_fixed": ("brunel_fixed", [70710, 70710], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1e9),
     # the generic kernel (window_ordered: every arrival through receive(), in order) on nets
     # the counting kernels also run, for comparison with the va and --syn 1e8 lines
+    # the reference's published single-GPU sizes (samples/main.cpp:1271-1294, results/bench.sh:26-28):
+    # VA at 1e9 synapses (p = 0.02, delay 8) and the sparse synth net (p = 0.00156, delay 1)
+    "va_1e9": ("vogels_abbott", [223607], [(0, 0, 0.02)], 8, 1e9),
+    "synth_1e9": ("synth", [800641], [(0, 0, 0.00156)], 1, 1e9),
     "va_ordered": ("vogels_abbott", [5000], [(0, 0, 0.02)], 1, 5000 * 5000 * 0.02),
     "brunel_ordered": ("brunel", [22360, 22360], [(0, 1, 0.1), (1, 1, 0.1)], 15, 1e8),
 }
 WORKLOAD_OPTIONS = {"va_ordered": {"kernel": "ordered"}, "brunel_ordered": {"kernel": "ordered"}}
+# the reference's published wall/bio for these workloads (its hardware, unstated)
+PUBLISHED = {"va_1e9": (1.08669, "results/spice.json:127"), "synth_1e9": (1.39947, "results/spice.json:31"),
+             "brunel_plus": (18.3537, "results/spice.json:367")}
 
 
 def parse():
@@ -62,7 +69,9 @@ def parse():
                          "serving: Poisson job arrivals, server vs plain per-job loop; va: Vogels-Abbott 4000+1000 "
                          "at delay 1; brunel_plus: Brunel with STDP at 5e8 synapses; va_ns, brunel_fixed, "
                          "brunel_plus_a012: the same with the benchmark configurations' model constants; "
-                         "va_ordered, brunel_ordered: VA and Brunel 1e8 on the generic window_ordered kernel")
+                         "va_ordered, brunel_ordered: VA and Brunel 1e8 on the generic window_ordered kernel; "
+                         "va_1e9, synth_1e9: the reference's published 1e9-synapse VA (delay 8) and sparse synth "
+                         "(delay 1) nets")
     ap.add_argument("--duration", type=float, default=8.0, help="serving: seconds of job arrivals")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: job arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
@@ -663,17 +672,21 @@ def run_model_workload(args, rank, world):
     if counts.sum():
         n = sum(pops)
         groups = {"exc": (0, int(0.8 * n)), "inh": (int(0.8 * n), n)} if model.startswith("vogels") else \
+                 {"all": (0, n)} if model == "synth" else \
                  {"poisson": (0, n // 2), "exc": (n // 2, int(0.9 * n)), "inh": (int(0.9 * n), n)}
         hist = np.bincount(ids, minlength=n)
         rates = {k: float(hist[a:b].sum()) / (b - a) / (steps * DT) for k, (a, b) in groups.items()}
     line["rates_hz"] = rates
+    if args.workload in PUBLISHED:
+        v, src = PUBLISHED[args.workload]
+        line["reference_published"] = {"value": v, "unit": "wall_s/bio_s", "source": src}
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
 
         small = syn > 1e7  # the CPU runs the full net only where it finishes in seconds
         reference_model = model in oracle.REFERENCE_MODELS
         fast = oracle.have_reference(fast=True) and reference_model
-        cpu_pops = [2000, 2000] if small else pops
+        cpu_pops = ([2000, 2000] if len(pops) == 2 else [4000]) if small else pops
         cpu_steps = 200 if small else steps
         mk = (lambda: oracle.ReferenceNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, fast=True)) if fast else \
              (lambda: oracle.OracleNet(model, cpu_pops, conns, dt=DT, delay=delay, seed=1, graph="reference", graph_seed=1337))

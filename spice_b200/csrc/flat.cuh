@@ -54,6 +54,10 @@ constexpr int FLAT_STEP_CAP = 1024;   // arrivals of one step the pipeline stage
 constexpr int FLAT_ENT_CAP = 6144;    // arrivals per segment of the synchronous path
 constexpr int FLAT_SCRATCH = 2560;    // per-(step, source tile) counts it stages at once (>= threads)
 constexpr int FLAT_MAX_TILE = 4064;   // slice lengths fit the table's 12-bit field
+// a slice is no longer than its row's ELL width either: nets of width <= FLAT_MAX_SLICE may
+// take tiles up to FLAT_MAX_TILE_WIDE (shared memory permitting)
+constexpr int FLAT_MAX_SLICE = 4095;
+constexpr int FLAT_MAX_TILE_WIDE = 16352;
 constexpr int FLAT_MIN_BUF = 512;     // vectors per buffer at least (one slice of a full tile)
 constexpr int FLAT_P_BITS = 20;       // vector offsets inside a step held in the table
 constexpr unsigned short SLICE_PAD = 0xFFFFu;

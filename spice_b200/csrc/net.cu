@@ -1057,15 +1057,24 @@ void set_tiles( spk_net & net, std::vector<int> const & first )
 // = the SM count for a net alone; fewer for a net that shares the GPU in a batch): the
 // tiles' first neurons and the shared-memory span of the largest tile with inputs; false
 // if the net does not fit window_flat.
-bool plan_flat(
-    int model, int device, long long n, std::vector<cost_segment> const & segs, int target, build_opts const & o, std::vector<int> & first, int & span, int & pack )
+bool plan_flat( int model,
+                int device,
+                long long n,
+                long long width,
+                std::vector<cost_segment> const & segs,
+                int target,
+                build_opts const & o,
+                std::vector<int> & first,
+                int & span,
+                int & pack )
 {
 	int optin = 0;
 	CK( cudaDeviceGetAttribute( &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device ) );
 	int const classes = classes_of( model ), attrs = neuron_attrs_of( model );
 	// largest tile whose counters, state, tables and minimal slice ring fit (with room for
 	// the kernel's static shared memory), and whose counter indices fit 16 bits
-	int tmax = spk::FLAT_MAX_TILE;
+	// a slice holds at most min(tile, row width) targets, and its length must fit 12 bits
+	int tmax = width <= spk::FLAT_MAX_SLICE ? spk::FLAT_MAX_TILE_WIDE : spk::FLAT_MAX_TILE;
 	while( tmax >= 128 && ( spk::flat_smem_bytes( classes, attrs, tmax ) + 4096 > (size_t)optin || (long long)classes * tmax >= spk::SLICE_PAD ) )
 		tmax -= 32;
 	// tiles without inputs keep only their neuron state and fired bits
@@ -1119,7 +1128,7 @@ bool flat_tiling( spk_net & net, std::vector<cost_segment> const & segs, int tar
 {
 	std::vector<int> first;
 	int span = 0, pack = 8;
-	if( !plan_flat( net.model, net.device, net.n, segs, target, net.opts, first, span, pack ) ) return false;
+	if( !plan_flat( net.model, net.device, net.n, net.width, segs, target, net.opts, first, span, pack ) ) return false;
 	net.flat = true;
 	net.pack = pack;
 	net.flat_tmax = ( span + 31 ) / 32 * 32;
@@ -1431,7 +1440,7 @@ size_t estimate_bytes( int model, spice::util::layout const & l, int delay, int 
 		int span = 0;
 		std::vector<cost_segment> const segs = layout_costs( l );
 		bool const per_step = o.kernel_auto && delay == 1 && segment_synapses( segs, n ) <= PER_STEP_MAX_SYNAPSES;
-		if( !o.direct && !per_step && plan_flat( model, device, n, segs, o.tile_target > 0 ? o.tile_target : sms, o, first, span, pack ) )
+		if( !o.direct && !per_step && plan_flat( model, device, n, w, segs, o.tile_target > 0 ? o.tile_target : sms, o, first, span, pack ) )
 		{
 			flat = true;
 			T = (long long)first.size() - 1;
@@ -1608,7 +1617,8 @@ void validate_checkpoint( ckpt_header const & h, std::vector<int> const & first,
 	else if( h.flat )
 	{
 		require( !plastic && T + 1 < spk::FLAT_PC && h.threads == spk::FLAT_THREADS && h.npt == 1 && h.tile == h.flat_tmax &&
-		             h.flat_tmax >= 32 && h.flat_tmax <= spk::FLAT_MAX_TILE && h.flat_tmax % 32 == 0,
+		             h.flat_tmax >= 32 && h.flat_tmax <= ( h.width <= spk::FLAT_MAX_SLICE ? spk::FLAT_MAX_TILE_WIDE : spk::FLAT_MAX_TILE ) &&
+		             h.flat_tmax % 32 == 0,
 		         "checkpoint tiling does not fit its kernel" );
 	}
 	else
